@@ -1,0 +1,264 @@
+"""cospdnn_b200 -- B200 (sm_100a) sparse-DNN inference engine, Python host side.
+
+Thin ctypes layer over the C ABI in include/cospdnn_b200.h (libcospdnn_b200.so,
+built in-tree by `python -m cospdnn_b200.build`).  There is no CPU fallback:
+every entry point raises if the CUDA library is missing or a call fails.
+
+Mirrors of the reference's operator surface (paths relative to CoSpDNN):
+  layer()                    <- ftxj::cospdnn_single       src/kernels/kernel.cuh:179-189
+  prune_compact()            <- check_active_f_col + host compaction + matrix_reshape
+                                src/kernels/kernel.cu:129-172, src/cospdnn.cu:236-276
+  test_graph_challenge_tc()  <- host layer loop           src/cospdnn.cuh:14-21
+  test_graph_challenge_tc_co() <- two-network loop        src/cospdnn.cuh:22-35
+  Engine                     <- both loops, any number of networks in one graph
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcospdnn_b200.so")
+
+# status codes (include/cospdnn_b200.h)
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_DEVICE, ERR_UNSUPPORTED = range(7)
+LAYER_A_FLOAT, LAYER_B_FLOAT, LAYER_REFERENCE_ARITH = 0x1, 0x2, 0x4
+PRUNE_OUT_HALF_HILO = 0x1
+PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
+KERNEL_AUTO, KERNEL_CUDA_CORE, KERNEL_TCGEN05 = 0, 1, 2
+INPUT_U8, INPUT_F32, INPUT_BITS = 0, 1, 2
+# bias table of the reference CLI (src/cospdnn.cpp:97-102)
+BIAS = {65536: -0.45, 16384: -0.4, 4096: -0.35, 1024: -0.3}
+THRESHOLD = 1e-5  # src/kernels/kernel.cu:133
+
+_lib = None
+
+
+class CospdnnError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cospdnn error {code}: {msg}")
+        self.code = code
+
+
+class NetDesc(C.Structure):
+    _fields_ = [("neuron", C.c_int), ("layers", C.c_int), ("rows", C.c_int), ("bias", C.c_float),
+                ("threshold", C.c_float), ("precision", C.c_int), ("kernel", C.c_int)]
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: build it with `python -m cospdnn_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, i32p, i64p, f32p = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int32), \
+            C.POINTER(C.c_int64), C.POINTER(C.c_float)
+        L.cospdnn_last_error.restype = C.c_char_p
+        L.cospdnn_version.restype = C.c_int
+        L.cospdnn_layer.argtypes = [vp, vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_uint, vp]
+        L.cospdnn_prune_workspace_bytes.restype = C.c_size_t
+        L.cospdnn_prune_workspace_bytes.argtypes = [C.c_int]
+        L.cospdnn_prune_compact.argtypes = [vp, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp,
+                                            C.c_uint, vp, C.c_size_t, vp]
+        L.cospdnn_engine_create.argtypes = [C.POINTER(vp), C.c_int]
+        L.cospdnn_engine_destroy.argtypes = [vp]
+        L.cospdnn_engine_destroy.restype = None
+        L.cospdnn_engine_add_net.argtypes = [vp, C.POINTER(NetDesc), ip]
+        L.cospdnn_engine_set_layer_csc.argtypes = [vp, C.c_int, C.c_int, i32p, i32p, f32p]
+        L.cospdnn_engine_set_layer_bcsc.argtypes = [vp, C.c_int, C.c_int, i32p, C.c_int, i32p,
+                                                    C.c_int, f32p, C.c_int, i32p]
+        L.cospdnn_engine_build.argtypes = [vp]
+        L.cospdnn_engine_set_input.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp]
+        L.cospdnn_engine_run.argtypes = [vp, vp]
+        L.cospdnn_engine_result.argtypes = [vp, C.c_int, i32p, i64p, i64p, i64p, vp]
+        L.cospdnn_engine_final_values.argtypes = [vp, C.c_int, f32p, C.c_int64, vp]
+        L.cospdnn_engine_launch_count.argtypes = [vp, i64p, vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise CospdnnError(rc, lib().cospdnn_last_error().decode())
+
+
+def _ptr(t):
+    """Device address of a torch tensor (or None)."""
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def _np(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+# ------------------------------------------------------------ layer entries
+def layer(A, B, C_out, fuse, idx_ptr, index, bias, batch, neuron, blocksize_c=16, blocksize_r=16,
+          nblockcols=None, flags=0, stream=None):
+    """cospdnn_single with the reference's argument meaning; torch CUDA tensors."""
+    if nblockcols is None:
+        nblockcols = idx_ptr.numel() - 1
+    _check(lib().cospdnn_layer(_ptr(A), _ptr(B), _ptr(C_out), _ptr(fuse), _ptr(idx_ptr),
+                               _ptr(index), float(bias), int(batch), int(neuron),
+                               int(blocksize_c), int(blocksize_r), int(nblockcols), int(flags),
+                               _stream(stream)))
+
+
+def prune_workspace_bytes(batch):
+    return int(lib().cospdnn_prune_workspace_bytes(int(batch)))
+
+
+def prune_compact(C_in, neuron, batch, threshold, A_out, category, map_in, map_out, count,
+                  workspace, flags=0, stream=None):
+    _check(lib().cospdnn_prune_compact(_ptr(C_in), int(neuron), int(batch), float(threshold),
+                                       _ptr(A_out), _ptr(category), _ptr(map_in), _ptr(map_out),
+                                       _ptr(count), int(flags), _ptr(workspace),
+                                       workspace.numel() * workspace.element_size(),
+                                       _stream(stream)))
+
+
+# ------------------------------------------------------------------ engine
+class Engine:
+    """Whole-network engine: add networks, set weights, build, then
+    set_input / run / result as often as needed."""
+
+    def __init__(self, device=0):
+        self._h = C.c_void_p()
+        _check(lib().cospdnn_engine_create(C.byref(self._h), int(device)))
+        self.nets = []
+
+    def close(self):
+        if self._h:
+            lib().cospdnn_engine_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_net(self, neuron, layers, rows, bias=None, threshold=THRESHOLD, precision=PREC_FP16,
+                kernel=KERNEL_AUTO):
+        if bias is None:
+            bias = BIAS[neuron]
+        d = NetDesc(int(neuron), int(layers), int(rows), float(bias), float(threshold),
+                    int(precision), int(kernel))
+        nid = C.c_int()
+        _check(lib().cospdnn_engine_add_net(self._h, C.byref(d), C.byref(nid)))
+        self.nets.append(dict(neuron=neuron, layers=layers, rows=rows, bias=bias))
+        return nid.value
+
+    def set_layer_csc(self, net, layer, colptr, rowidx, vals):
+        cp, ri, vv = _np(colptr, np.int32), _np(rowidx, np.int32), _np(vals, np.float32)
+        _check(lib().cospdnn_engine_set_layer_csc(
+            self._h, net, layer, cp.ctypes.data_as(C.POINTER(C.c_int32)),
+            ri.ctypes.data_as(C.POINTER(C.c_int32)), vv.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def set_layer_bcsc(self, net, layer, col_ptr, row_index, values, blocksize=16, fuse=None):
+        cp, ri, vv = _np(col_ptr, np.int32), _np(row_index, np.int32), _np(values, np.float32)
+        fz = None if fuse is None else _np(fuse, np.int32)
+        _check(lib().cospdnn_engine_set_layer_bcsc(
+            self._h, net, layer, cp.ctypes.data_as(C.POINTER(C.c_int32)), len(cp),
+            ri.ctypes.data_as(C.POINTER(C.c_int32)), len(ri),
+            vv.ctypes.data_as(C.POINTER(C.c_float)), int(blocksize),
+            None if fz is None else fz.ctypes.data_as(C.POINTER(C.c_int32))))
+
+    def build(self):
+        _check(lib().cospdnn_engine_build(self._h))
+
+    def set_input(self, net, y0, fmt=None, stream=None):
+        """y0: numpy array (host; pinned memory not required) or torch CUDA
+        tensor; uint8 -> INPUT_U8, float32 -> INPUT_F32 unless fmt given."""
+        on_device = hasattr(y0, "data_ptr") and getattr(y0, "is_cuda", False)
+        if on_device:
+            ptr = C.c_void_p(y0.data_ptr())
+            dt = str(y0.dtype)
+        else:
+            if not hasattr(y0, "ctypes"):
+                y0 = np.asarray(y0)
+            if not y0.flags["C_CONTIGUOUS"]:
+                y0 = np.ascontiguousarray(y0)
+            self._keep = y0
+            ptr = C.c_void_p(y0.ctypes.data)
+            dt = str(y0.dtype)
+        if fmt is None:
+            fmt = INPUT_U8 if "uint8" in dt else INPUT_F32
+        _check(lib().cospdnn_engine_set_input(self._h, net, ptr, int(fmt), int(on_device),
+                                              _stream(stream)))
+
+    def run(self, stream=None):
+        _check(lib().cospdnn_engine_run(self._h, _stream(stream)))
+
+    def result(self, net, stream=None):
+        info = self.nets[net]
+        cats = np.empty(max(1, info["rows"]), np.int32)
+        alive = np.zeros(info["layers"], np.int64)
+        rech = np.zeros(info["layers"], np.int64)
+        cnt = C.c_int64()
+        _check(lib().cospdnn_engine_result(
+            self._h, net, cats.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(cnt),
+            alive.ctypes.data_as(C.POINTER(C.c_int64)), rech.ctypes.data_as(C.POINTER(C.c_int64)),
+            _stream(stream)))
+        return dict(categories=cats[:cnt.value].copy(), alive=alive, rechecked=rech)
+
+    def final_values(self, net, max_rows, stream=None):
+        out = np.empty((max(1, max_rows), self.nets[net]["neuron"]), np.float32)
+        _check(lib().cospdnn_engine_final_values(self._h, net,
+                                                 out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 int(max_rows), _stream(stream)))
+        return out[:max_rows]
+
+    def launch_count(self, stream=None):
+        v = C.c_int64()
+        _check(lib().cospdnn_engine_launch_count(self._h, C.byref(v), _stream(stream)))
+        return v.value
+
+
+# ------------------------------------------------- reference host API mirror
+def test_graph_challenge_tc(input, weight, row_idx, ptr, fuse_list, batch, neuron, bias,
+                            blocksize_c=16, blocksize_r=16, gpu_id=0, gpu_num=1,
+                            precision=PREC_FP16, threshold=THRESHOLD, verbose=True):
+    """Mirror of the reference's test_graph_challenge_tc (src/cospdnn.cu:3-369).
+
+    input      [batch][neuron] values (numpy; binary images in the Graph Challenge)
+    weight     per layer: BCSC block values (bcsc_values_)
+    row_idx    per layer: block start rows (bcsc_row_index_)
+    ptr        per layer: block-column pointer (bcsc_len_)
+    fuse_list  per layer: activation row of each weight row (or None)
+    Runs every layer on GPU `gpu_id` (rows split over gpu_num slices as in
+    src/cospdnn.cu:23,35-44, this call computing slice gpu_id).  Prints the
+    reference's per-layer "layer l, feature = n" lines when verbose and
+    returns dict(categories, alive).  Raises on error instead of exiting.
+    """
+    rows_per = (batch + gpu_num - 1) // gpu_num
+    lo, hi = gpu_id * rows_per, min((gpu_id + 1) * rows_per, batch)
+    x = np.asarray(input)[lo:hi]
+    L = len(weight)
+    eng = Engine(gpu_id if gpu_num > 1 else 0)
+    try:
+        net = eng.add_net(neuron, L, hi - lo, bias, threshold, precision)
+        for l in range(L):
+            if blocksize_c != blocksize_r:
+                raise CospdnnError(ERR_UNSUPPORTED, "square blocks only")
+            fz = None if fuse_list is None else fuse_list[l]
+            eng.set_layer_bcsc(net, l, ptr[l], row_idx[l], weight[l], blocksize_c, fz)
+        eng.build()
+        eng.set_input(net, x.astype(np.uint8) if np.all((x == 0) | (x == 1)) else
+                      x.astype(np.float32))
+        eng.run()
+        res = eng.result(net)
+    finally:
+        eng.close()
+    if verbose:
+        for l, n in enumerate(res["alive"]):
+            print(f"layer {l}, feature = {n}")
+    res["categories"] = res["categories"] + lo
+    return res

@@ -1,0 +1,690 @@
+// Whole-network engine: host side (setup, graph capture, C ABI) plus the
+// input conversion kernel.  Replaces the host layer loops of the reference
+// (src/cospdnn.cu:3-369, src/cospdnn_double.cu:208-1214).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "engine_kernels.cuh"
+#include "tc_layer.cuh"
+
+namespace cospdnn {
+
+namespace {
+
+// ---- input conversion: any format -> compute type, per-row error and max --
+template <typename T, int FMT>
+__global__ void k_convert_input(const void *__restrict__ src, int rows, int N, T *__restrict__ y0,
+                                float *__restrict__ y0_f32, float *__restrict__ err0,
+                                float *__restrict__ mx0) {
+    // one warp per row
+    const int lane = threadIdx.x & 31;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = w; r < rows; r += nw) {
+        float e = 0.0f, m = 0.0f;
+        for (int j = lane; j < N; j += 32) {
+            float x;
+            if (FMT == COSPDNN_INPUT_U8) x = (float)((const uint8_t *)src)[r * N + j];
+            else if (FMT == COSPDNN_INPUT_F32) x = ((const float *)src)[r * N + j];
+            else x = (float)((((const uint8_t *)src)[r * (N / 8) + (j >> 3)] >> (j & 7)) & 1u);
+            const T v = act_traits<T>::from_f(x);
+            y0[r * N + j] = v;
+            if (y0_f32) y0_f32[r * N + j] = x;
+            e = fmaxf(e, fabsf(act_traits<T>::to_f(v) - x));
+            m = fmaxf(m, fabsf(x));
+        }
+        e = warp_max(e);
+        m = warp_max(m);
+        if (lane == 0) {
+            err0[r] = e;
+            mx0[r] = m;
+        }
+    }
+}
+
+// gather of the final activations (checks only)
+template <typename T>
+__global__ void k_gather_final(const NetDev *__restrict__ nd_p, float *__restrict__ out, int64_t max_rows) {
+    const NetDev &nd = *nd_p;
+    const int R = nd.st->R, par = nd.st->layer & 1, N = nd.N;
+    const T *act = (const T *)nd.act[par];
+    const int64_t total = (int64_t)min((int64_t)R, max_rows) * N;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = i / N, j = i % N;
+        out[i] = act_traits<T>::to_f(act[(int64_t)nd.pos[par][q] * N + j]);
+    }
+}
+
+size_t elem_size(int prec) { return prec == COSPDNN_PREC_FP32 ? 4 : 2; }
+
+template <typename T>
+T *dalloc(size_t n, std::vector<void *> &owned) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    owned.push_back(p);
+    return (T *)p;
+}
+
+float to_compute(float w, int prec) {
+    if (prec == COSPDNN_PREC_FP16) return __half2float(__float2half_rn(w));
+    if (prec == COSPDNN_PREC_BF16) return __bfloat162float(__float2bfloat16_rn(w));
+    return w;
+}
+
+struct HostLayer {
+    std::vector<int32_t> colptr, rowidx;
+    std::vector<float> vals;
+    bool set = false;
+};
+
+struct Net {
+    cospdnn_net_desc d{};
+    std::vector<HostLayer> layers;
+    NetDev dev{};
+    std::vector<LayerDev> ldev;
+    LayerDev *d_layers = nullptr;
+    void *staging = nullptr;
+    size_t staging_bytes = 0;
+    float *y0_f32 = nullptr;
+};
+
+}  // namespace
+
+thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t err, const char *what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(err);
+    return err == cudaErrorMemoryAllocation ? COSPDNN_ERR_NOMEM : COSPDNN_ERR_CUDA;
+}
+
+}  // namespace cospdnn
+
+using namespace cospdnn;
+
+struct cospdnn_engine {
+    int device = 0;
+    std::vector<Net> nets;
+    std::vector<void *> owned;
+    bool built = false;
+    NetDev *d_nets = nullptr;
+    int max_n = 0, max_layers = 0;
+    double *scratch = nullptr;
+    int replay_ctas = 0;
+    unsigned long long *launches = nullptr;
+    unsigned int *finished = nullptr;
+    int *loop_guard = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle loop{};
+    KSpec k0, k2, k3, k4_graph, k4_eager;
+    std::vector<KSpec> layer_specs;
+    std::vector<long long *> packbuf;  // per net: device buffer for result_async
+    ~cospdnn_engine() {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void *p : owned) cudaFree(p);
+        cudaSetDevice(cur);
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
+    const HostLayer &h = net.layers[l];
+    const int N = net.d.neuron;
+    int K = 1;
+    for (int j = 0; j < N; ++j) K = std::max(K, h.colptr[j + 1] - h.colptr[j]);
+    std::vector<int32_t> idx((size_t)K * N, 0);
+    std::vector<float> val((size_t)K * N, 0.0f);
+    double S = 0.0, dW = 0.0;
+    for (int j = 0; j < N; ++j) {
+        double s = 0.0, d = 0.0;
+        for (int p = h.colptr[j], k = 0; p < h.colptr[j + 1]; ++p, ++k) {
+            idx[(size_t)k * N + j] = h.rowidx[p];
+            val[(size_t)k * N + j] = h.vals[p];
+            const float wc = to_compute(h.vals[p], net.d.precision);
+            s += std::max(std::fabs((double)h.vals[p]), std::fabs((double)wc));
+            d += std::fabs((double)wc - (double)h.vals[p]);
+        }
+        S = std::max(S, s);
+        dW = std::max(dW, d);
+    }
+    int32_t *didx = dalloc<int32_t>(idx.size(), e->owned);
+    float *dval = dalloc<float>(val.size(), e->owned);
+    CSP_CHECK(didx && dval, COSPDNN_ERR_NOMEM, "engine: weight allocation failed");
+    CSP_CUDA(cudaMemcpy(didx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice));
+    CSP_CUDA(cudaMemcpy(dval, val.data(), val.size() * 4, cudaMemcpyHostToDevice));
+    ld = LayerDev{};
+    ld.ell_idx = didx;
+    ld.ell_val = dval;
+    ld.K = K;
+    ld.S = (float)(S * (1.0 + 1e-7));
+    ld.dW = (float)(dW * (1.0 + 1e-7));
+    if (net.dev.kernel == COSPDNN_KERNEL_TCGEN05) {
+        int rc = tc_build_blocks(h.colptr, h.rowidx, h.vals, N, net.d.precision, ld, e->owned);
+        if (rc) return rc;
+    }
+    return COSPDNN_OK;
+}
+
+int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std::vector<int> &tc_precs) {
+    int sms = 148;
+    CSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+    const int nn = (int)e->nets.size();
+    NetDev *nets = e->d_nets;
+    unsigned long long *launches = e->launches;
+    int *guard = e->loop_guard;
+    KSpec &k0 = e->k0;
+    k0.fn = (void *)k_init_run;
+    k0.grid = dim3(sms * 4);
+    k0.block = dim3(256);
+    k0.arg(nets).arg(nn).arg(launches).arg(guard);
+    for (int prec : plain_precs) {
+        KSpec k;
+        k.fn = prec == COSPDNN_PREC_FP32 ? (void *)k_layer_plain<float>
+             : prec == COSPDNN_PREC_FP16 ? (void *)k_layer_plain<__half>
+                                         : (void *)k_layer_plain<__nv_bfloat16>;
+        int per_sm = 0;
+        CSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, kPlainThreads, 0));
+        k.grid = dim3(sms * std::max(1, per_sm));
+        k.block = dim3(kPlainThreads);
+        k.arg(nets).arg(nn).arg(prec).arg(launches);
+        e->layer_specs.push_back(std::move(k));
+    }
+    for (int prec : tc_precs) {
+        KSpec k;
+        int rc = tc_layer_spec(k, nets, nn, prec, launches, sms);
+        if (rc) return rc;
+        e->layer_specs.push_back(std::move(k));
+    }
+    KSpec &k2 = e->k2;
+    k2.fn = (void *)k_classify;
+    k2.grid = dim3(sms * 4);
+    k2.block = dim3(256);
+    k2.arg(nets).arg(nn).arg(launches);
+    KSpec &k3 = e->k3;
+    k3.fn = (void *)k_replay;
+    k3.grid = dim3(e->replay_ctas);
+    k3.block = dim3(kReplayThreads);
+    k3.arg(nets).arg(nn).arg(e->scratch).arg(e->max_n).arg(launches);
+    for (int use_cond = 0; use_cond < 2; ++use_cond) {
+        KSpec &k4 = use_cond ? e->k4_graph : e->k4_eager;
+        k4.fn = (void *)k_compact;
+        k4.grid = dim3(nn);
+        k4.block = dim3(kCompactThreads);
+        k4.arg(nets).arg(nn).arg(e->finished).arg(e->loop).arg(use_cond).arg(guard)
+            .arg(e->max_layers + 2).arg(launches);
+    }
+    return COSPDNN_OK;
+}
+
+int add_node(cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, int ndeps, KSpec &k) {
+    cudaKernelNodeParams p{};
+    p.func = k.fn;
+    p.gridDim = k.grid;
+    p.blockDim = k.block;
+    p.sharedMemBytes = (unsigned)k.smem;
+    p.kernelParams = k.params();
+    CSP_CUDA(cudaGraphAddKernelNode(node, g, deps, ndeps, &p));
+    return COSPDNN_OK;
+}
+
+int launch(KSpec &k, cudaStream_t s) {
+    CSP_CUDA(cudaLaunchKernel(k.fn, k.grid, k.block, k.params(), k.smem, s));
+    return COSPDNN_OK;
+}
+
+int build_graph(cospdnn_engine *e, const std::vector<int> &plain_precs, const std::vector<int> &tc_precs) {
+    CSP_CUDA(cudaGraphCreate(&e->graph, 0));
+    CSP_CUDA(cudaGraphConditionalHandleCreate(&e->loop, e->graph, 1, cudaGraphCondAssignDefault));
+    int rc = make_specs(e, plain_precs, tc_precs);
+    if (rc) return rc;
+    cudaGraphNode_t k0;
+    if ((rc = add_node(e->graph, &k0, nullptr, 0, e->k0))) return rc;
+    // while (any network live) { layer kernels; classify; FP64 replay; compact }
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = e->loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CSP_CUDA(cudaGraphAddNode(&cnode, e->graph, &k0, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    std::vector<cudaGraphNode_t> layer_nodes(e->layer_specs.size());
+    for (size_t i = 0; i < e->layer_specs.size(); ++i)
+        if ((rc = add_node(body, &layer_nodes[i], nullptr, 0, e->layer_specs[i]))) return rc;
+    cudaGraphNode_t k2, k3, k4;
+    if ((rc = add_node(body, &k2, layer_nodes.data(), (int)layer_nodes.size(), e->k2))) return rc;
+    if ((rc = add_node(body, &k3, &k2, 1, e->k3))) return rc;
+    if ((rc = add_node(body, &k4, &k3, 1, e->k4_graph))) return rc;
+    CSP_CUDA(cudaGraphInstantiate(&e->exec, e->graph, 0));
+    return COSPDNN_OK;
+}
+
+}  // namespace
+
+extern "C" const char *cospdnn_last_error(void) { return g_err.c_str(); }
+extern "C" int cospdnn_version(void) { return 100; }
+
+extern "C" int cospdnn_engine_create(cospdnn_engine **out, int device) {
+    CSP_CHECK(out, COSPDNN_ERR_INVALID, "engine_create: null out");
+    int ndev = 0;
+    CSP_CUDA(cudaGetDeviceCount(&ndev));
+    CSP_CHECK(device >= 0 && device < ndev, COSPDNN_ERR_INVALID, "engine_create: no such device");
+    cudaDeviceProp prop;
+    CSP_CUDA(cudaGetDeviceProperties(&prop, device));
+    CSP_CHECK(prop.major == 10 && prop.minor == 0, COSPDNN_ERR_UNSUPPORTED,
+              "engine_create: this library is built for sm_100a (B200) only");
+    auto *e = new (std::nothrow) cospdnn_engine();
+    CSP_CHECK(e, COSPDNN_ERR_NOMEM, "engine_create: out of host memory");
+    e->device = device;
+    *out = e;
+    return COSPDNN_OK;
+}
+
+extern "C" void cospdnn_engine_destroy(cospdnn_engine *e) { delete e; }
+
+extern "C" int cospdnn_engine_add_net(cospdnn_engine *e, const cospdnn_net_desc *d, int *net_id) {
+    CSP_CHECK(e && d, COSPDNN_ERR_INVALID, "add_net: null argument");
+    CSP_CHECK(!e->built, COSPDNN_ERR_STATE, "add_net: engine already built");
+    CSP_CHECK(d->neuron > 0 && d->layers > 0 && d->rows >= 0, COSPDNN_ERR_INVALID, "add_net: bad sizes");
+    CSP_CHECK(d->precision >= 0 && d->precision <= 2, COSPDNN_ERR_INVALID, "add_net: bad precision");
+    CSP_CHECK(d->kernel >= 0 && d->kernel <= 2, COSPDNN_ERR_INVALID, "add_net: bad kernel");
+    CSP_CHECK(!(d->kernel == COSPDNN_KERNEL_TCGEN05 && d->precision == COSPDNN_PREC_FP32),
+              COSPDNN_ERR_UNSUPPORTED, "add_net: tcgen05 kernel needs FP16 or BF16");
+    CSP_CHECK(d->threshold >= 0.0f && d->threshold < 32.0f, COSPDNN_ERR_INVALID, "add_net: threshold outside [0,32)");
+    Net net;
+    net.d = *d;
+    net.layers.resize(d->layers);
+    int k = d->kernel;
+    if (k == COSPDNN_KERNEL_AUTO)
+        k = (d->precision != COSPDNN_PREC_FP32 && tc_supported(d->neuron)) ? COSPDNN_KERNEL_TCGEN05
+                                                                         : COSPDNN_KERNEL_CUDA_CORE;
+    if (k == COSPDNN_KERNEL_TCGEN05)
+        CSP_CHECK(tc_supported(d->neuron), COSPDNN_ERR_UNSUPPORTED, "add_net: tcgen05 kernel needs neuron % 16 == 0");
+    net.dev.kernel = k;
+    e->nets.push_back(std::move(net));
+    if (net_id) *net_id = (int)e->nets.size() - 1;
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_set_layer_csc(cospdnn_engine *e, int net, int layer,
+                                            const int32_t *colptr, const int32_t *rowidx,
+                                            const float *vals) {
+    CSP_CHECK(e && colptr, COSPDNN_ERR_INVALID, "set_layer_csc: null argument");
+    CSP_CHECK(!e->built, COSPDNN_ERR_STATE, "set_layer_csc: engine already built");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "set_layer_csc: bad net");
+    Net &n = e->nets[net];
+    CSP_CHECK(layer >= 0 && layer < n.d.layers, COSPDNN_ERR_INVALID, "set_layer_csc: bad layer");
+    const int N = n.d.neuron;
+    CSP_CHECK(colptr[0] == 0, COSPDNN_ERR_INVALID, "set_layer_csc: colptr[0] != 0");
+    for (int j = 0; j < N; ++j)
+        CSP_CHECK(colptr[j + 1] >= colptr[j], COSPDNN_ERR_INVALID, "set_layer_csc: colptr not monotone");
+    const int64_t nnz = colptr[N];
+    CSP_CHECK(nnz == 0 || (rowidx && vals), COSPDNN_ERR_INVALID, "set_layer_csc: null rowidx/vals");
+    for (int j = 0; j < N; ++j)
+        for (int p = colptr[j]; p < colptr[j + 1]; ++p) {
+            CSP_CHECK(rowidx[p] >= 0 && rowidx[p] < N, COSPDNN_ERR_INVALID, "set_layer_csc: row index out of range");
+            CSP_CHECK(p == colptr[j] || rowidx[p] > rowidx[p - 1], COSPDNN_ERR_INVALID,
+                      "set_layer_csc: rows must be strictly ascending within a column");
+            CSP_CHECK(std::isfinite(vals[p]), COSPDNN_ERR_INVALID, "set_layer_csc: non-finite weight");
+        }
+    HostLayer &h = n.layers[layer];
+    h.colptr.assign(colptr, colptr + N + 1);
+    h.rowidx.assign(rowidx, rowidx + nnz);
+    h.vals.assign(vals, vals + nnz);
+    h.set = true;
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_set_layer_bcsc(cospdnn_engine *e, int net, int layer,
+                                             const int32_t *col_ptr, int n_col_ptr,
+                                             const int32_t *row_index, int n_blocks,
+                                             const float *values, int blocksize,
+                                             const int32_t *fuse) {
+    CSP_CHECK(e && col_ptr && row_index && values, COSPDNN_ERR_INVALID, "set_layer_bcsc: null argument");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "set_layer_bcsc: bad net");
+    const int N = e->nets[net].d.neuron;
+    CSP_CHECK(blocksize > 0 && n_col_ptr >= 1 && n_blocks >= 0, COSPDNN_ERR_INVALID, "set_layer_bcsc: bad sizes");
+    CSP_CHECK(col_ptr[0] == 0 && col_ptr[n_col_ptr - 1] == n_blocks, COSPDNN_ERR_INVALID,
+              "set_layer_bcsc: col_ptr does not span the blocks");
+    // fold: W[fuse[start+ro]][bid*bs+co] += V[co*bs+ro]
+    std::vector<std::vector<std::pair<int32_t, float>>> cols(N);
+    const int64_t bsz = (int64_t)blocksize * blocksize;
+    for (int bid = 0; bid + 1 < n_col_ptr; ++bid) {
+        CSP_CHECK(col_ptr[bid + 1] >= col_ptr[bid], COSPDNN_ERR_INVALID, "set_layer_bcsc: col_ptr not monotone");
+        for (int blk = col_ptr[bid]; blk < col_ptr[bid + 1]; ++blk) {
+            for (int co = 0; co < blocksize; ++co) {
+                const int o = bid * blocksize + co;
+                for (int ro = 0; ro < blocksize; ++ro) {
+                    const float v = values[blk * bsz + (int64_t)co * blocksize + ro];
+                    if (v == 0.0f) continue;
+                    const int r = row_index[blk] + ro;
+                    CSP_CHECK(o < N && r >= 0 && r < N, COSPDNN_ERR_INVALID, "set_layer_bcsc: nonzero outside the matrix");
+                    const int a = fuse ? fuse[r] : r;
+                    CSP_CHECK(a >= 0 && a < N, COSPDNN_ERR_INVALID, "set_layer_bcsc: fuse entry out of range");
+                    cols[o].push_back({a, v});
+                }
+            }
+        }
+    }
+    std::vector<int32_t> cp(N + 1, 0), ri;
+    std::vector<float> vv;
+    for (int j = 0; j < N; ++j) {
+        auto &c = cols[j];
+        std::sort(c.begin(), c.end(), [](const std::pair<int32_t, float> &x, const std::pair<int32_t, float> &y) {
+            return x.first < y.first;
+        });
+        for (size_t t = 0; t < c.size(); ++t) {
+            if (!ri.empty() && (int)ri.size() > cp[j] && ri.back() == c[t].first) vv.back() += c[t].second;
+            else { ri.push_back(c[t].first); vv.push_back(c[t].second); }
+        }
+        cp[j + 1] = (int32_t)ri.size();
+    }
+    return cospdnn_engine_set_layer_csc(e, net, layer, cp.data(), ri.data(), vv.data());
+}
+
+extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
+    CSP_CHECK(e, COSPDNN_ERR_INVALID, "build: null engine");
+    CSP_CHECK(!e->built, COSPDNN_ERR_STATE, "build: already built");
+    CSP_CHECK(!e->nets.empty(), COSPDNN_ERR_STATE, "build: no networks");
+    DeviceGuard g(e->device);
+    std::vector<int> plain, tc;
+    for (Net &n : e->nets) {
+        for (int l = 0; l < n.d.layers; ++l)
+            CSP_CHECK(n.layers[l].set, COSPDNN_ERR_STATE, "build: a layer's weights were not set");
+        e->max_n = std::max(e->max_n, n.d.neuron);
+        e->max_layers = std::max(e->max_layers, n.d.layers);
+        auto &v = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? tc : plain;
+        if (std::find(v.begin(), v.end(), n.d.precision) == v.end()) v.push_back(n.d.precision);
+    }
+    for (Net &n : e->nets) {
+        const int N = n.d.neuron, R = std::max(1, n.d.rows);
+        n.ldev.resize(n.d.layers);
+        for (int l = 0; l < n.d.layers; ++l) {
+            int rc = upload_layer(e, n, l, n.ldev[l]);
+            if (rc) return rc;
+            n.layers[l] = HostLayer();  // host copy no longer needed
+            n.layers[l].set = true;
+        }
+        n.d_layers = dalloc<LayerDev>(n.d.layers, e->owned);
+        CSP_CHECK(n.d_layers, COSPDNN_ERR_NOMEM, "build: allocation failed");
+        CSP_CUDA(cudaMemcpy(n.d_layers, n.ldev.data(), sizeof(LayerDev) * n.d.layers, cudaMemcpyHostToDevice));
+        NetDev &d = n.dev;
+        d.N = N;
+        d.L = n.d.layers;
+        d.rows = n.d.rows;
+        d.prec = n.d.precision;
+        d.bias = n.d.bias;
+        d.tau = n.d.threshold;
+        d.layers = n.d_layers;
+        const size_t es = elem_size(d.prec), act = (size_t)R * N * es;
+        d.y0 = dalloc<char>(act, e->owned);
+        d.act[0] = dalloc<char>(act, e->owned);
+        d.act[1] = dalloc<char>(act, e->owned);
+        float *err0 = dalloc<float>(R, e->owned), *mx0 = dalloc<float>(R, e->owned);
+        d.err0 = err0;
+        d.mx0 = mx0;
+        for (int b = 0; b < 2; ++b) {
+            d.pos[b] = dalloc<int32_t>(R, e->owned);
+            d.orig[b] = dalloc<int32_t>(R, e->owned);
+            d.err[b] = dalloc<float>(R, e->owned);
+            d.mx[b] = dalloc<float>(R, e->owned);
+        }
+        d.stat = dalloc<uint32_t>((size_t)3 * R, e->owned);
+        d.cls = dalloc<int8_t>(R, e->owned);
+        d.ulist = dalloc<int32_t>(R, e->owned);
+        d.alive_count = dalloc<long long>(d.L, e->owned);
+        d.recheck_count = dalloc<long long>(d.L, e->owned);
+        d.st = dalloc<NetState>(1, e->owned);
+        CSP_CHECK(d.y0 && d.act[0] && d.act[1] && err0 && mx0 && d.pos[0] && d.pos[1] && d.orig[0] &&
+                      d.orig[1] && d.err[0] && d.err[1] && d.mx[0] && d.mx[1] && d.stat && d.cls &&
+                      d.ulist && d.alive_count && d.recheck_count && d.st,
+                  COSPDNN_ERR_NOMEM, "build: device allocation failed");
+        CSP_CUDA(cudaMemset((void *)d.y0, 0, act));
+        CSP_CUDA(cudaMemset(err0, 0, sizeof(float) * R));
+        CSP_CUDA(cudaMemset(mx0, 0, sizeof(float) * R));
+        CSP_CUDA(cudaMemset(d.st, 0, sizeof(NetState)));
+    }
+    for (Net &n : e->nets) {
+        long long *pb = dalloc<long long>(1 + n.d.layers + (std::max(1, n.d.rows) + 1) / 2, e->owned);
+        CSP_CHECK(pb, COSPDNN_ERR_NOMEM, "build: allocation failed");
+        e->packbuf.push_back(pb);
+    }
+    e->d_nets = dalloc<NetDev>(e->nets.size(), e->owned);
+    CSP_CHECK(e->d_nets, COSPDNN_ERR_NOMEM, "build: allocation failed");
+    for (size_t i = 0; i < e->nets.size(); ++i)
+        CSP_CUDA(cudaMemcpy(e->d_nets + i, &e->nets[i].dev, sizeof(NetDev), cudaMemcpyHostToDevice));
+    int sms = 148;
+    CSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+    e->replay_ctas = 2 * sms;
+    e->scratch = dalloc<double>((size_t)e->replay_ctas * 2 * e->max_n, e->owned);
+    e->launches = dalloc<unsigned long long>(1, e->owned);
+    e->finished = dalloc<unsigned int>(1, e->owned);
+    e->loop_guard = dalloc<int>(1, e->owned);
+    CSP_CHECK(e->scratch && e->launches && e->finished && e->loop_guard, COSPDNN_ERR_NOMEM,
+              "build: allocation failed");
+    CSP_CUDA(cudaMemset(e->finished, 0, sizeof(unsigned int)));
+    CSP_CUDA(cudaMemset(e->launches, 0, sizeof(unsigned long long)));
+    int rc = build_graph(e, plain, tc);
+    if (rc) return rc;
+    CSP_CUDA(cudaDeviceSynchronize());
+    e->built = true;
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *y0, int format,
+                                        int on_device, void *stream) {
+    CSP_CHECK(e && y0, COSPDNN_ERR_INVALID, "set_input: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "set_input: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "set_input: bad net");
+    CSP_CHECK(format >= 0 && format <= 2, COSPDNN_ERR_INVALID, "set_input: bad format");
+    DeviceGuard g(e->device);
+    Net &n = e->nets[net];
+    const int N = n.d.neuron, R = n.d.rows;
+    if (R == 0) return COSPDNN_OK;
+    CSP_CHECK(format != COSPDNN_INPUT_BITS || N % 8 == 0, COSPDNN_ERR_INVALID, "set_input: bit rows need neuron % 8 == 0");
+    const size_t bytes = format == COSPDNN_INPUT_U8 ? (size_t)R * N
+                       : format == COSPDNN_INPUT_F32 ? (size_t)R * N * 4 : (size_t)R * (N / 8);
+    cudaStream_t s = (cudaStream_t)stream;
+    const void *src = y0;
+    if (!on_device) {
+        if (n.staging_bytes < bytes) {
+            if (n.staging) cudaFree(n.staging);
+            n.staging = nullptr;
+            n.staging_bytes = 0;
+            CSP_CUDA(cudaMalloc(&n.staging, bytes));
+            e->owned.push_back(n.staging);
+            n.staging_bytes = bytes;
+        }
+        CSP_CUDA(cudaMemcpyAsync(n.staging, y0, bytes, cudaMemcpyHostToDevice, s));
+        src = n.staging;
+    }
+    float *f32 = nullptr;
+    if (format == COSPDNN_INPUT_F32 && n.d.precision != COSPDNN_PREC_FP32) {
+        if (!n.y0_f32) {
+            CSP_CUDA(cudaMalloc(&n.y0_f32, (size_t)R * N * 4));
+            e->owned.push_back(n.y0_f32);
+        }
+        f32 = n.y0_f32;
+    }
+    if (n.dev.y0_f32 != f32) {
+        n.dev.y0_f32 = f32;
+        CSP_CUDA(cudaMemcpyAsync(&e->d_nets[net].y0_f32, &n.dev.y0_f32, sizeof(float *), cudaMemcpyHostToDevice, s));
+        CSP_CUDA(cudaStreamSynchronize(s));
+    }
+    const int blocks = std::min(65535, (R + 7) / 8);
+    float *err0 = (float *)n.dev.err0, *mx0 = (float *)n.dev.mx0;
+#define CSP_CONV(T)                                                                                      \
+    do {                                                                                                 \
+        T *dst = (T *)n.dev.y0;                                                                          \
+        if (format == COSPDNN_INPUT_U8) k_convert_input<T, COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, R, N, dst, f32, err0, mx0); \
+        else if (format == COSPDNN_INPUT_F32) k_convert_input<T, COSPDNN_INPUT_F32><<<blocks, 256, 0, s>>>(src, R, N, dst, f32, err0, mx0); \
+        else k_convert_input<T, COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, R, N, dst, f32, err0, mx0); \
+    } while (0)
+    if (n.d.precision == COSPDNN_PREC_FP32) CSP_CONV(float);
+    else if (n.d.precision == COSPDNN_PREC_FP16) CSP_CONV(__half);
+    else CSP_CONV(__nv_bfloat16);
+#undef CSP_CONV
+    CSP_CUDA(cudaGetLastError());
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_run(cospdnn_engine *e, void *stream) {
+    CSP_CHECK(e, COSPDNN_ERR_INVALID, "run: null engine");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "run: build first");
+    DeviceGuard g(e->device);
+    CSP_CUDA(cudaGraphLaunch(e->exec, (cudaStream_t)stream));
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_result(cospdnn_engine *e, int net, int32_t *categories, int64_t *count,
+                                     int64_t *alive_per_layer, int64_t *rechecked_per_layer,
+                                     void *stream) {
+    CSP_CHECK(e && count, COSPDNN_ERR_INVALID, "result: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "result: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "result: bad net");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    Net &n = e->nets[net];
+    NetState st;
+    CSP_CUDA(cudaMemcpyAsync(&st, n.dev.st, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CSP_CUDA(cudaStreamSynchronize(s));
+    CSP_CHECK(st.err == 0, COSPDNN_ERR_DEVICE, "result: device-side loop guard tripped");
+    CSP_CHECK(st.done, COSPDNN_ERR_STATE, "result: network has not finished (run first)");
+    const int64_t cnt = (st.layer >= n.d.layers) ? st.R : 0;
+    *count = cnt;
+    if (categories && cnt > 0)
+        CSP_CUDA(cudaMemcpyAsync(categories, n.dev.orig[st.layer & 1], sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, s));
+    std::vector<long long> tmp(n.d.layers);
+    if (alive_per_layer) {
+        CSP_CUDA(cudaMemcpyAsync(tmp.data(), n.dev.alive_count, sizeof(long long) * n.d.layers, cudaMemcpyDeviceToHost, s));
+        CSP_CUDA(cudaStreamSynchronize(s));
+        for (int l = 0; l < n.d.layers; ++l) alive_per_layer[l] = tmp[l];
+    }
+    if (rechecked_per_layer) {
+        CSP_CUDA(cudaMemcpyAsync(tmp.data(), n.dev.recheck_count, sizeof(long long) * n.d.layers, cudaMemcpyDeviceToHost, s));
+        CSP_CUDA(cudaStreamSynchronize(s));
+        for (int l = 0; l < n.d.layers; ++l) rechecked_per_layer[l] = tmp[l];
+    }
+    CSP_CUDA(cudaStreamSynchronize(s));
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_final_values(cospdnn_engine *e, int net, float *out, int64_t max_rows,
+                                           void *stream) {
+    CSP_CHECK(e && out, COSPDNN_ERR_INVALID, "final_values: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "final_values: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "final_values: bad net");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    Net &n = e->nets[net];
+    const size_t bytes = (size_t)std::max<int64_t>(1, std::min<int64_t>(max_rows, n.d.rows)) * n.d.neuron * 4;
+    float *tmp = nullptr;
+    CSP_CUDA(cudaMalloc(&tmp, bytes));
+    if (n.d.precision == COSPDNN_PREC_FP32) k_gather_final<float><<<592, 256, 0, s>>>(e->d_nets + net, tmp, max_rows);
+    else if (n.d.precision == COSPDNN_PREC_FP16) k_gather_final<__half><<<592, 256, 0, s>>>(e->d_nets + net, tmp, max_rows);
+    else k_gather_final<__nv_bfloat16><<<592, 256, 0, s>>>(e->d_nets + net, tmp, max_rows);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    CSP_CUDA(err);
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_launch_count(cospdnn_engine *e, int64_t *launches, void *stream) {
+    CSP_CHECK(e && launches, COSPDNN_ERR_INVALID, "launch_count: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "launch_count: build first");
+    DeviceGuard g(e->device);
+    unsigned long long v = 0;
+    CSP_CUDA(cudaMemcpyAsync(&v, e->launches, sizeof(v), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CSP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    *launches = (int64_t)v;
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_result_async(cospdnn_engine *e, int net, void *host_buf, size_t bytes,
+                                           void *stream) {
+    CSP_CHECK(e && host_buf, COSPDNN_ERR_INVALID, "result_async: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "result_async: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "result_async: bad net");
+    const Net &n = e->nets[net];
+    const size_t need = 8 * (size_t)(1 + n.d.layers) + 4 * (size_t)n.d.rows;
+    CSP_CHECK(bytes >= need, COSPDNN_ERR_INVALID, "result_async: buffer too small");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    k_result_pack<<<8, 256, 0, s>>>(e->d_nets + net, e->packbuf[net]);
+    CSP_CUDA(cudaGetLastError());
+    CSP_CUDA(cudaMemcpyAsync(host_buf, e->packbuf[net], need, cudaMemcpyDeviceToHost, s));
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, int max_iters,
+                                             float *layer_ms, int *iters) {
+    CSP_CHECK(e && layer_ms && iters && max_iters > 0, COSPDNN_ERR_INVALID, "profile_layers: bad argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "profile_layers: build first");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t a, b;
+    CSP_CUDA(cudaEventCreate(&a));
+    CSP_CUDA(cudaEventCreate(&b));
+    int rc = launch(e->k0, s);
+    int it = 0;
+    std::vector<NetState> st(e->nets.size());
+    while (!rc && it < max_iters) {
+        bool live = false;
+        for (size_t i = 0; i < e->nets.size() && !rc; ++i) {
+            cudaError_t err = cudaMemcpyAsync(&st[i], e->nets[i].dev.st, sizeof(NetState), cudaMemcpyDeviceToHost, s);
+            if (err != cudaSuccess) rc = cuda_fail(err, "profile_layers: state copy");
+        }
+        if (rc) break;
+        cudaError_t err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) { rc = cuda_fail(err, "profile_layers: sync"); break; }
+        for (auto &x : st) live |= !x.done;
+        if (!live) break;
+        cudaEventRecord(a, s);
+        for (KSpec &k : e->layer_specs) if (!rc) rc = launch(k, s);
+        cudaEventRecord(b, s);
+        if (!rc) rc = launch(e->k2, s);
+        if (!rc) rc = launch(e->k3, s);
+        if (!rc) rc = launch(e->k4_eager, s);
+        if (rc) break;
+        err = cudaEventSynchronize(b);
+        if (err != cudaSuccess) { rc = cuda_fail(err, "profile_layers: event"); break; }
+        cudaEventElapsedTime(&layer_ms[it], a, b);
+        ++it;
+    }
+    *iters = it;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (!rc) {
+        cudaError_t err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) rc = cuda_fail(err, "profile_layers: final sync");
+    }
+    return rc;
+}

@@ -1,0 +1,366 @@
+// Kernels of the device-driven layer loop.  Every kernel reads the per-net
+// state (current layer, active rows) from device memory, so one captured graph
+// serves every layer and every network; grids are fixed and loop over the
+// work that the state describes.
+#pragma once
+
+#include "engine.cuh"
+
+namespace cospdnn {
+
+__device__ __forceinline__ void count_launch(unsigned long long *launches) {
+    if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+}
+
+// ---- K0: start of a run --------------------------------------------------
+__global__ void k_init_run(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches,
+                           int *loop_guard) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (launches) *launches = 1ull;
+        *loop_guard = 0;
+    }
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    for (int n = 0; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        if (tid == 0) {
+            nd.st->layer = 0;
+            nd.st->R = nd.rows;
+            nd.st->done = (nd.rows == 0 || nd.L == 0);
+            nd.st->nunc = 0;
+            nd.st->err = 0;
+        }
+        for (int64_t l = tid; l < nd.L; l += nth) {
+            nd.alive_count[l] = 0;
+            nd.recheck_count[l] = 0;
+        }
+        for (int64_t p = tid; p < nd.rows; p += nth) {
+            nd.pos[0][p] = (int32_t)p;
+            nd.orig[0][p] = (int32_t)p;
+            nd.err[0][p] = nd.err0[p];
+            nd.mx[0][p] = nd.mx0[p];
+            nd.stat[3 * p] = 0u;
+            nd.stat[3 * p + 1] = 0u;
+            nd.stat[3 * p + 2] = 0u;
+        }
+    }
+}
+
+// ---- K1 (CUDA cores): one warp = 4 rows x all outputs ---------------------
+// Lane j of a 32-output segment accumulates output j of 4 rows over the ELL
+// entries of column j (index and weight loaded once, used for 4 rows), then
+// applies bias + clamp, stores the compute-type value and folds the output into
+// the row statistics (max z, error bound of the stored outputs, max output).
+constexpr int kPlainRows = 4;
+constexpr int kPlainThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kPlainThreads)
+    k_layer_plain(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
+    count_launch(launches);
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    // units of kPlainRows rows, enumerated net after net
+    int64_t total = 0;
+    for (int n = 0; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        if (nd.kernel != COSPDNN_KERNEL_CUDA_CORE || nd.prec != prec || nd.st->done) continue;
+        total += (nd.st->R + kPlainRows - 1) / kPlainRows;
+    }
+    for (int64_t unit = gwarp; unit < total; unit += nwarps) {
+        int64_t u = unit;
+        int n = 0;
+        for (; n < nnets; ++n) {
+            const NetDev &nd = nets[n];
+            if (nd.kernel != COSPDNN_KERNEL_CUDA_CORE || nd.prec != prec || nd.st->done) continue;
+            const int64_t cnt = (nd.st->R + kPlainRows - 1) / kPlainRows;
+            if (u < cnt) break;
+            u -= cnt;
+        }
+        const NetDev &nd = nets[n];
+        const int N = nd.N, l = nd.st->layer, R = nd.st->R, par = l & 1;
+        const LayerDev lw = nd.layers[l];
+        const T *in = (const T *)(l == 0 ? nd.y0 : nd.act[par]);
+        T *out = (T *)nd.act[par ^ 1];
+        const double steps = fast_steps(nd, lw);
+        const T *inrow[kPlainRows];
+        T *outrow[kPlainRows];
+        float ez[kPlainRows], zmax[kPlainRows], emax[kPlainRows], ymax[kPlainRows];
+        bool valid[kPlainRows];
+#pragma unroll
+        for (int r = 0; r < kPlainRows; ++r) {
+            const int p = (int)(u * kPlainRows) + r;
+            valid[r] = p < R;
+            const int pp = valid[r] ? p : (int)(u * kPlainRows);
+            inrow[r] = in + (int64_t)nd.pos[par][pp] * N;
+            outrow[r] = out + (int64_t)pp * N;
+            ez[r] = z_error_bound(nd.err[par][pp], nd.mx[par][pp], lw.S, lw.dW, nd.bias, steps);
+            zmax[r] = -INFINITY;
+            emax[r] = 0.0f;
+            ymax[r] = 0.0f;
+        }
+        for (int j0 = 0; j0 < N; j0 += 32) {
+            const int j = j0 + lane;
+            if (j < N) {
+                float acc[kPlainRows];
+#pragma unroll
+                for (int r = 0; r < kPlainRows; ++r) acc[r] = 0.0f;
+                const int32_t *ip = lw.ell_idx + j;
+                const float *wp = lw.ell_val + j;
+                for (int k = 0; k < lw.K; ++k) {
+                    const int32_t i = __ldg(ip + (int64_t)k * N);
+                    const float w = __ldg(wp + (int64_t)k * N);
+#pragma unroll
+                    for (int r = 0; r < kPlainRows; ++r)
+                        acc[r] = fmaf(w, act_traits<T>::to_f(inrow[r][i]), acc[r]);
+                }
+#pragma unroll
+                for (int r = 0; r < kPlainRows; ++r) {
+                    const float z = acc[r] + nd.bias;
+                    const float c = clamp32(z);
+                    const T ys = act_traits<T>::from_f(c);
+                    const float yf = act_traits<T>::to_f(ys);
+                    if (valid[r]) outrow[r][j] = ys;
+                    zmax[r] = fmaxf(zmax[r], z);
+                    ymax[r] = fmaxf(ymax[r], yf);
+                    if (z > -ez[r] && z < 32.0f + ez[r]) emax[r] = fmaxf(emax[r], __fadd_ru(ez[r], fabsf(yf - c)));
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kPlainRows; ++r) {
+            const float zm = warp_max(zmax[r]), em = warp_max(emax[r]), ym = warp_max(ymax[r]);
+            if (lane == 0 && valid[r]) {
+                const int p = (int)(u * kPlainRows) + r;
+                nd.stat[3 * p] = f2ord(zm);
+                nd.stat[3 * p + 1] = __float_as_uint(em);
+                nd.stat[3 * p + 2] = __float_as_uint(ym);
+            }
+        }
+    }
+}
+
+// ---- K2: keep / prune / uncertain per row ---------------------------------
+__global__ void k_classify(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
+    count_launch(launches);
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    for (int n = 0; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        if (nd.st->done) continue;
+        const int l = nd.st->layer, R = nd.st->R, par = l & 1;
+        const LayerDev &lw = nd.layers[l];
+        const double steps = fast_steps(nd, lw);
+        for (int64_t p = tid; p < R; p += nth) {
+            const float zm = ord2f(nd.stat[3 * p]);
+            const float ez = z_error_bound(nd.err[par][p], nd.mx[par][p], lw.S, lw.dW, nd.bias, steps);
+            const double lo = (double)zm - (double)ez, hi = (double)zm + (double)ez;
+            int8_t c;
+            if (lo > (double)nd.tau) c = CLS_KEEP;
+            else if (hi <= (double)nd.tau) c = CLS_PRUNE;
+            else c = CLS_UNCERTAIN;
+            nd.cls[p] = c;
+            if (c == CLS_UNCERTAIN) nd.ulist[atomicAdd(&nd.st->nunc, 1)] = (int32_t)p;
+        }
+    }
+}
+
+// ---- K3: exact FP64 replay of uncertain rows ------------------------------
+// One CTA per uncertain row: recompute the row from its exact input through
+// the current layer in the oracle's order (for each output, ascending input
+// index, separately rounded multiply and add, bias last, clamp), decide
+// keep/prune exactly, and for kept rows overwrite the fast output with the
+// FP64 values rounded to the compute type.
+constexpr int kReplayThreads = 256;
+
+__device__ __forceinline__ float block_max(float v, float *red) {
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? red[lane] : -INFINITY;
+        v = warp_max(v);
+        if (lane == 0) red[0] = v;
+    }
+    __syncthreads();
+    return red[0];
+}
+
+template <typename T>
+__device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, float *red) {
+    const int N = nd.N, l = nd.st->layer, par = l & 1;
+    const int orow = nd.orig[par][p];
+    double *y = buf0, *z = buf1;
+    for (int j = threadIdx.x; j < N; j += blockDim.x)
+        y[j] = nd.y0_f32 ? (double)nd.y0_f32[(int64_t)orow * N + j]
+                         : act_traits<T>::to_d(((const T *)nd.y0)[(int64_t)orow * N + j]);
+    __syncthreads();
+    const double b = (double)nd.bias;
+    for (int ll = 0; ll <= l; ++ll) {
+        const LayerDev &lw = nd.layers[ll];
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            double acc = 0.0;
+            for (int k = 0; k < lw.K; ++k) {
+                const double yi = y[lw.ell_idx[(int64_t)k * N + j]];
+                if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)lw.ell_val[(int64_t)k * N + j], yi));
+            }
+            z[j] = clamp32d(__dadd_rn(acc, b));
+        }
+        __syncthreads();
+        double *t = y; y = z; z = t;
+    }
+    // y holds the layer-l outputs
+    float zmax = 0.0f, emax = 0.0f, ymax = 0.0f;
+    double dmax = 0.0;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) dmax = fmax(dmax, y[j]);
+    // exact keep decision on the FP64 values
+    zmax = block_max(dmax > (double)nd.tau ? 1.0f : 0.0f, red);
+    const bool keep = zmax > 0.5f;
+    if (keep) {
+        T *out = (T *)nd.act[par ^ 1] + (int64_t)p * N;
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const T v = act_traits<T>::from_d(y[j]);
+            out[j] = v;
+            const double vd = act_traits<T>::to_d(v);
+            emax = fmaxf(emax, __double2float_ru(fabs(vd - y[j])));
+            ymax = fmaxf(ymax, (float)vd);
+        }
+        emax = block_max(emax, red);
+        ymax = block_max(ymax, red);
+    }
+    if (threadIdx.x == 0) {
+        nd.cls[p] = keep ? CLS_KEEP : CLS_PRUNE;
+        if (keep) {
+            nd.stat[3 * p + 1] = __float_as_uint(emax);
+            nd.stat[3 * p + 2] = __float_as_uint(ymax);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kReplayThreads)
+    k_replay(const NetDev *__restrict__ nets, int nnets, double *__restrict__ scratch, int max_n,
+             unsigned long long *launches) {
+    count_launch(launches);
+    __shared__ float red[32];
+    double *b0 = scratch + (int64_t)blockIdx.x * 2 * max_n;
+    double *b1 = b0 + max_n;
+    int64_t total = 0;
+    for (int n = 0; n < nnets; ++n)
+        if (!nets[n].st->done) total += nets[n].st->nunc;
+    for (int64_t q = blockIdx.x; q < total; q += gridDim.x) {
+        int64_t u = q;
+        int n = 0;
+        for (; n < nnets; ++n) {
+            if (nets[n].st->done) continue;
+            if (u < nets[n].st->nunc) break;
+            u -= nets[n].st->nunc;
+        }
+        const NetDev &nd = nets[n];
+        const int p = nd.ulist[u];
+        if (nd.prec == COSPDNN_PREC_FP32) replay_row<float>(nd, p, b0, b1, red);
+        else if (nd.prec == COSPDNN_PREC_FP16) replay_row<__half>(nd, p, b0, b1, red);
+        else replay_row<__nv_bfloat16>(nd, p, b0, b1, red);
+    }
+}
+
+// ---- K4: stable compaction + state advance + loop condition ---------------
+constexpr int kCompactThreads = 1024;
+
+__global__ void __launch_bounds__(kCompactThreads)
+    k_compact(const NetDev *__restrict__ nets, int nnets, unsigned int *finished_ctas,
+              cudaGraphConditionalHandle loop, int use_cond, int *loop_guard, int max_iters,
+              unsigned long long *launches) {
+    count_launch(launches);
+    __shared__ int warp_tot[kCompactThreads / 32];
+    __shared__ int carry, s_done, s_layer, s_R;
+    const int n = blockIdx.x;
+    const NetDev &nd = nets[n];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        s_done = nd.st->done;
+        s_layer = nd.st->layer;
+        s_R = nd.st->R;
+        carry = 0;
+    }
+    __syncthreads();
+    if (!s_done) {
+        const int l = s_layer, R = s_R, par = l & 1;
+        for (int base = 0; base < R; base += kCompactThreads) {
+            const int p = base + threadIdx.x;
+            const int keep = (p < R && nd.cls[p] == CLS_KEEP) ? 1 : 0;
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 31) warp_tot[wid] = __popc(m);
+            __syncthreads();
+            if (wid == 0) {
+                int v = warp_tot[lane];
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane >= o) v += t;
+                }
+                warp_tot[lane] = v;
+            }
+            __syncthreads();
+            if (keep) {
+                const int q = carry + (wid ? warp_tot[wid - 1] : 0) + __popc(m & ((1u << lane) - 1u));
+                nd.pos[par ^ 1][q] = p;
+                nd.orig[par ^ 1][q] = nd.orig[par][p];
+                nd.err[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 1]);
+                nd.mx[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 2]);
+            }
+            if (p < R) {
+                nd.stat[3 * p] = 0u;
+                nd.stat[3 * p + 1] = 0u;
+                nd.stat[3 * p + 2] = 0u;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) carry += warp_tot[kCompactThreads / 32 - 1];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            nd.alive_count[l] = carry;
+            nd.recheck_count[l] = nd.st->nunc;
+            nd.st->nunc = 0;
+            nd.st->R = carry;
+            nd.st->layer = l + 1;
+            nd.st->done = (carry == 0 || l + 1 >= nd.L);
+        }
+    }
+    // the last CTA to finish decides whether the graph loop runs again
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned done_ctas = atomicAdd(finished_ctas, 1u) + 1u;
+        if (done_ctas == (unsigned)gridDim.x) {
+            *finished_ctas = 0u;
+            __threadfence();
+            int live = 0;
+            for (int i = 0; i < nnets; ++i) live |= !(*(volatile int *)&nets[i].st->done);
+            const int it = ++*loop_guard;
+            if (it > max_iters) {
+                for (int i = 0; i < nnets; ++i) nets[i].st->err = COSPDNN_ERR_DEVICE;
+                live = 0;
+            }
+            if (use_cond) cudaGraphSetConditional(loop, live ? 1u : 0u);
+        }
+    }
+}
+
+// ---- packed result for asynchronous copies --------------------------------
+// buf: int64 count, int64 alive[L], int32 categories[rows]
+__global__ void k_result_pack(const NetDev *__restrict__ nd_p, long long *__restrict__ buf) {
+    const NetDev &nd = *nd_p;
+    const int layer = nd.st->layer, R = nd.st->R;
+    const int cnt = (nd.st->done && layer >= nd.L) ? R : 0;
+    int32_t *cats = (int32_t *)(buf + 1 + nd.L);
+    const int32_t *src = nd.orig[layer & 1];
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    if (tid == 0) buf[0] = cnt;
+    for (int l = tid; l < nd.L; l += nth) buf[1 + l] = nd.alive_count[l];
+    for (int q = tid; q < cnt; q += nth) cats[q] = src[q];
+}
+
+}  // namespace cospdnn

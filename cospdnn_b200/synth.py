@@ -1,0 +1,129 @@
+"""Seeded synthetic networks in the shapes of the Graph Challenge sparse DNNs.
+
+Weights W_l: 32 distinct masks m_k drawn uniformly from [0, N) per (net,
+layer); W[i][i ^ m_k] = 1/16, i.e. exactly 32 nonzeros per row and column.
+Inputs Y0: binary rows, row r with density U[dlo, dhi), generated on the GPU
+(cospdnn_synth_input).  Streams are SplitMix64 (Steele, Lea & Flood 2014):
+stream_seed(seed, kind, net, x) with kind 1 = masks (x = layer), 2 = input
+rows (x = row), 3 = the multi-network mix, 4 = reference-compatible masks.
+Also writes the reference's file formats (src/cospdnn.cpp:14-79).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+M64 = (1 << 64) - 1
+GAMMA = 0x9E3779B97F4A7C15
+
+
+def _mix(z):
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+    return z ^ (z >> 31)
+
+
+class SplitMix64:
+    def __init__(self, state):
+        self.s = state & M64
+
+    def next(self):
+        self.s = (self.s + GAMMA) & M64
+        return _mix(self.s)
+
+
+def stream_seed(seed, a, b, c):
+    g = SplitMix64(seed ^ 0x5851F42D4C957F2D)
+    x = g.next()
+    g.s = x ^ ((a + 0x632BE59BD9B4E019) & M64)
+    x = g.next()
+    g.s = x ^ ((b + 0x9E3779B97F4A7C15) & M64)
+    x = g.next()
+    g.s = x ^ ((c + 0xD1B54A32D192ED03) & M64)
+    return g.next()
+
+
+def xor_masks(seed, net, layer, neuron, nmask=32):
+    g = SplitMix64(stream_seed(seed, 1, net, layer))
+    out = []
+    while len(out) < nmask:
+        m = g.next() % neuron
+        if m not in out:
+            out.append(m)
+    return np.array(out, np.int32)
+
+
+def r1_masks(seed, net, layer, neuron):
+    """Masks {16*h0+t, 16*h1+t}: two aligned dense 16x16 blocks per block column."""
+    nb = neuron // 16
+    g = SplitMix64(stream_seed(seed, 4, net, layer))
+    h0 = g.next() % nb
+    h1 = g.next() % nb
+    while h1 == h0:
+        h1 = g.next() % nb
+    return np.array([16 * h0 + t for t in range(16)] + [16 * h1 + t for t in range(16)], np.int32)
+
+
+def masks_to_csc(masks, neuron, val=0.0625):
+    """CSC (row = input, column = output): output j <- inputs j ^ m_k, ascending."""
+    masks = np.asarray(masks, np.int64)
+    j = np.arange(neuron, dtype=np.int64)[:, None]
+    rows = np.sort(j ^ masks[None, :], axis=1).astype(np.int32)
+    k = len(masks)
+    colptr = (np.arange(neuron + 1, dtype=np.int64) * k).astype(np.int32)
+    return colptr, rows.reshape(-1), np.full(neuron * k, val, np.float32)
+
+
+def mix_config(seed, nnet=8, nchoices=(1024, 4096, 16384), lchoices=(120, 480), bmin=2000,
+               bmax=60000):
+    g = SplitMix64(stream_seed(seed, 3, 0, 0))
+    out = []
+    for _ in range(nnet):
+        n = nchoices[g.next() % len(nchoices)]
+        l = lchoices[g.next() % len(lchoices)]
+        b = bmin + g.next() % (bmax - bmin + 1)
+        out.append((int(n), int(l), int(b)))
+    return out
+
+
+def network(neuron, layers, seed, net=0, kind="xor"):
+    """List of per-layer CSC triplets."""
+    f = r1_masks if kind == "r1" else xor_masks
+    return [masks_to_csc(f(seed, net, l, neuron), neuron) for l in range(layers)]
+
+
+def input_rows(rows, neuron, seed, net=0, dlo=0.08, dhi=0.25, row0=0, fmt=0, device=0, stream=None):
+    """Binary inputs generated on the GPU; returns a torch uint8 CUDA tensor
+    [rows][neuron] (fmt 0) or packed bits [rows][neuron/8] (fmt 2)."""
+    import torch
+
+    from . import _check, _stream, lib
+    cols = neuron if fmt == 0 else neuron // 8
+    out = torch.empty((rows, cols), dtype=torch.uint8, device=f"cuda:{device}")
+    f = lib().cospdnn_synth_input
+    f.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.c_int64, C.c_double,
+                  C.c_double, C.c_int, C.c_void_p]
+    _check(f(out.data_ptr(), rows, neuron, seed, net, row0, dlo, dhi, fmt, _stream(stream)))
+    return out
+
+
+# ---------------------------------------------------------- reference files
+def write_reference_dataset(dirname, neuron, layers, y0, csc_layers, fuse=None):
+    """Writes dir/sparse-images-N.tsv, dir/neuronN/N-l{l+1}.tsv and
+    dir/fuse_matrix/neuronN/N_L_fuse.tsv in the reference's formats."""
+    os.makedirs(os.path.join(dirname, f"neuron{neuron}"), exist_ok=True)
+    os.makedirs(os.path.join(dirname, "fuse_matrix", f"neuron{neuron}"), exist_ok=True)
+    r, c = np.nonzero(np.asarray(y0))
+    with open(os.path.join(dirname, f"sparse-images-{neuron}.tsv"), "w") as f:
+        for a, b in zip((r + 1).tolist(), (c + 1).tolist()):
+            f.write(f"{a}\t{b}\t1\n")
+    for l, (cp, ri, vv) in enumerate(csc_layers):
+        col = np.repeat(np.arange(neuron), np.diff(cp))
+        with open(os.path.join(dirname, f"neuron{neuron}", f"{neuron}-l{l + 1}.tsv"), "w") as f:
+            for a, b, v in zip((ri + 1).tolist(), (col + 1).tolist(), vv.tolist()):
+                f.write(f"{a}\t{b}\t{v:.6g}\n")
+    with open(os.path.join(dirname, "fuse_matrix", f"neuron{neuron}",
+                           f"{neuron}_{layers}_fuse.tsv"), "w") as f:
+        for l in range(layers):
+            row = np.arange(neuron) if fuse is None else fuse[l]
+            f.write("\t".join(str(int(x)) for x in row) + "\n")

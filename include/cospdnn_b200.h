@@ -1,0 +1,190 @@
+/*
+ * cospdnn_b200 -- C ABI of the B200 (sm_100a) sparse-DNN inference engine.
+ *
+ * Plain pointers and sizes only.  Every function returns a status code
+ * (COSPDNN_OK == 0) instead of exiting the process as the reference's
+ * Safe_Call does (src/gpu_lib/gpu_runtime.h:6-17); cospdnn_last_error()
+ * gives the message of the calling thread's last failure.  Device pointers
+ * are CUDA device memory of the current device; `stream` is a cudaStream_t
+ * (NULL = legacy default stream).  Reference paths are relative to the
+ * CoSpDNN repository.
+ */
+#ifndef COSPDNN_B200_H
+#define COSPDNN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    COSPDNN_OK = 0,
+    COSPDNN_ERR_INVALID = 1,     /* bad argument */
+    COSPDNN_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    COSPDNN_ERR_NOMEM = 3,       /* device or host allocation failed */
+    COSPDNN_ERR_STATE = 4,       /* call out of order (e.g. run before build) */
+    COSPDNN_ERR_DEVICE = 5,      /* a device-side check failed (bounds, loop guard) */
+    COSPDNN_ERR_UNSUPPORTED = 6  /* shape or option this build does not handle */
+};
+
+/* Message of the calling thread's last failing call ("" if none). */
+const char *cospdnn_last_error(void);
+/* Library version as major*10000 + minor*100 + patch. */
+int cospdnn_version(void);
+
+/* ------------------------------------------------------------------------
+ * Layer entry.  Replaces ftxj::cospdnn_single (src/kernels/kernel.cuh:179-189,
+ * launched at src/cospdnn.cu:219-229) with the same argument meaning:
+ *   A        activations, feature-major, batch contiguous:
+ *            default: half [2*neuron][batch], rows 0..neuron-1 the hi parts and
+ *            rows neuron..2*neuron-1 the lo parts (src/kernels/kernel.cu:140-152);
+ *            COSPDNN_LAYER_A_FLOAT: float [neuron][batch].
+ *   B        block values, blocksize_c*blocksize_r per block, value
+ *            [col_off*blocksize_c + row_off] (src/utils/matrix.h:1245);
+ *            half by default (src/cospdnn.cu:46-56), float with COSPDNN_LAYER_B_FLOAT.
+ *   C        float [neuron][batch], every row of every block column written.
+ *   fuse     activation row of each weight row (src/cospdnn.cpp:14-44).
+ *   idx_ptr  block-column pointer (bcsc_len_), nblockcols+1 entries.
+ *   index    start row of each block (bcsc_row_index_).
+ *   Output column o = bid*blocksize_c + col_off (block columns are taken as
+ *   blocksize_c-aligned, as the reference kernel's output indexing does).
+ * Default arithmetic: the true product over every block of the column,
+ *   C[o][b] = clamp(bias + sum_blocks sum_ro V[co*bc+ro] * A[fuse[start+ro]][b], 0, 32),
+ *   hi+lo summed, FP32 accumulation; weight rows >= neuron are skipped.
+ * COSPDNN_LAYER_REFERENCE_ARITH reproduces the reference kernel's arithmetic
+ *   instead: only the two blocks starting at idx_ptr[bid], and value
+ *   [k*16 + r] applied from input row start+k to output bid*16+r
+ *   (src/kernels/kernel.cu:257,306-331,371-375); requires blocksize 16.
+ * batch need not be a multiple of 128.  Asynchronous on `stream`.
+ */
+#define COSPDNN_LAYER_A_FLOAT 0x1u
+#define COSPDNN_LAYER_B_FLOAT 0x2u
+#define COSPDNN_LAYER_REFERENCE_ARITH 0x4u
+int cospdnn_layer(const void *A, const void *B, float *C, const int *fuse, const int *idx_ptr,
+                  const int *index, float bias, int batch, int neuron, int blocksize_c,
+                  int blocksize_r, int nblockcols, unsigned flags, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Pruning entry.  Replaces check_active_f_col (src/kernels/kernel.cu:129-139),
+ * the host compaction loop (src/cospdnn.cu:240-270) and matrix_reshape
+ * (src/kernels/kernel.cu:156-172) with one device-side pass, no host round trip:
+ *   column k of C ([neuron][batch] float) survives if any C[n][k] > threshold
+ *   (the reference uses 1e-5);
+ *   survivors keep ascending order: category[j] = k of the j-th survivor,
+ *   map_out[j] = map_in[k] (map_in NULL = identity), *count_dev = survivors;
+ *   A_out [neuron][stride], stride = count rounded up to a multiple of 128,
+ *   gets the surviving columns and zero padding; with COSPDNN_PRUNE_OUT_HALF_HILO
+ *   A_out is half [2*neuron][stride] hi/lo rows, ready for cospdnn_layer.
+ * A_out, category and map_out need room for batch columns.  `workspace` is
+ * device memory of cospdnn_prune_workspace_bytes(batch) bytes, owned by the
+ * caller.  Asynchronous; read *count_dev after synchronizing.
+ */
+#define COSPDNN_PRUNE_OUT_HALF_HILO 0x1u
+size_t cospdnn_prune_workspace_bytes(int batch);
+int cospdnn_prune_compact(const float *C, int neuron, int batch, float threshold, void *A_out,
+                          int *category, const int *map_in, int *map_out, int *count_dev,
+                          unsigned flags, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Whole-network engine.  Replaces the host layer loop test_graph_challenge_tc
+ * (src/cospdnn.cu:3-369) and the two-network path test_graph_challenge_tc_co
+ * (src/cospdnn_double.cu:208-1214): any number of networks of any sizes run
+ * in one captured CUDA graph whose device-side loop advances every live
+ * network by one layer per iteration and stops when all are finished.
+ * Each network computes Y_{l+1} = clamp(Y_l W_l + bias, 0, 32); a row is
+ * pruned after the first layer whose outputs are all <= threshold; the
+ * categories are the original ids of the rows alive after the last layer.
+ * Rows whose keep/prune decision is within the proven error bound of the
+ * fast precision are re-decided by an exact FP64 replay from Y0, so the
+ * categories equal those of the FP64 recurrence.
+ */
+typedef struct cospdnn_engine cospdnn_engine;
+
+#define COSPDNN_PREC_FP32 0 /* FP32 activations, CUDA-core kernel */
+#define COSPDNN_PREC_FP16 1 /* FP16 activations, FP32 accumulation */
+#define COSPDNN_PREC_BF16 2 /* BF16 activations, FP32 accumulation */
+
+#define COSPDNN_KERNEL_AUTO 0      /* tensor cores for FP16/BF16, CUDA cores for FP32 */
+#define COSPDNN_KERNEL_CUDA_CORE 1 /* gather-FMA kernel, any precision */
+#define COSPDNN_KERNEL_TCGEN05 2   /* tcgen05 block MMA kernel (FP16/BF16) */
+
+typedef struct {
+    int neuron;      /* features per layer */
+    int layers;      /* number of layers */
+    int rows;        /* input rows (batch) */
+    float bias;      /* bias of every neuron (reference table src/cospdnn.cpp:97-102) */
+    float threshold; /* prune rule: row alive if any output > threshold (reference 1e-5) */
+    int precision;   /* COSPDNN_PREC_* */
+    int kernel;      /* COSPDNN_KERNEL_* */
+} cospdnn_net_desc;
+
+int cospdnn_engine_create(cospdnn_engine **out, int device);
+void cospdnn_engine_destroy(cospdnn_engine *e);
+int cospdnn_engine_add_net(cospdnn_engine *e, const cospdnn_net_desc *d, int *net_id);
+/* W_l in CSC form (row = input, column = output; src/utils/matrix.h:282-289),
+ * host arrays, rows ascending within each column. */
+int cospdnn_engine_set_layer_csc(cospdnn_engine *e, int net, int layer, const int32_t *colptr,
+                                 const int32_t *rowidx, const float *vals);
+/* W_l in the reference's BCSC form (host arrays from BCSRCSCMatrix, values
+ * [col_off*bs + row_off]) plus the layer's fuse row (NULL = identity).  Block
+ * value [co*bs + ro] of block column bid is the weight from activation row
+ * fuse[start + ro] to output bid*bs + co (the true product of cospdnn_layer's
+ * default arithmetic); the engine folds the fuse into its own weight layout. */
+int cospdnn_engine_set_layer_bcsc(cospdnn_engine *e, int net, int layer, const int32_t *col_ptr,
+                                  int n_col_ptr, const int32_t *row_index, int n_blocks,
+                                  const float *values, int blocksize, const int32_t *fuse);
+/* Uploads weights, allocates every device buffer and captures the CUDA graph. */
+int cospdnn_engine_build(cospdnn_engine *e);
+
+#define COSPDNN_INPUT_U8 0   /* [rows][neuron] bytes (binary images) */
+#define COSPDNN_INPUT_F32 1  /* [rows][neuron] float */
+#define COSPDNN_INPUT_BITS 2 /* [rows][neuron/8] bytes, bit j%8 of byte j/8, LSB first */
+/* Copies Y0 of one network (host pointer: pinned memory keeps it async).
+ * Asynchronous on `stream`. */
+int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *y0, int format,
+                             int on_device, void *stream);
+/* Runs every network to completion: one graph launch, asynchronous. */
+int cospdnn_engine_run(cospdnn_engine *e, void *stream);
+/* Synchronizes `stream`, then copies results of one network to host memory:
+ * categories (ascending original row ids, room for `rows`), their count,
+ * alive rows after each layer (room for `layers`, may be NULL) and rows
+ * re-decided in FP64 at each layer (may be NULL). */
+int cospdnn_engine_result(cospdnn_engine *e, int net, int32_t *categories, int64_t *count,
+                          int64_t *alive_per_layer, int64_t *rechecked_per_layer, void *stream);
+/* Copies the activations of the last computed layer for the surviving rows
+ * (in category order) into a host float buffer [count][neuron]; for checks. */
+int cospdnn_engine_final_values(cospdnn_engine *e, int net, float *out, int64_t max_rows,
+                                void *stream);
+/* Number of launches of this library's kernels the last run made (device
+ * counter, read after synchronizing). */
+int cospdnn_engine_launch_count(cospdnn_engine *e, int64_t *launches, void *stream);
+/* Asynchronous result copy for end-to-end pipelines: after the run on `stream`,
+ * packs one network's result and copies it to host_buf (pinned memory keeps it
+ * asynchronous): int64 count, int64 alive_per_layer[layers], int32
+ * categories[rows].  Needs 8*(1+layers) + 4*rows bytes. */
+int cospdnn_engine_result_async(cospdnn_engine *e, int net, void *host_buf, size_t bytes,
+                                void *stream);
+/* Runs the same kernels as cospdnn_engine_run layer by layer from the host
+ * (synchronizing after each layer) and times the layer kernels of each
+ * iteration with CUDA events on `stream`: layer_ms[i] for iteration i (all
+ * networks advance one layer per iteration), up to max_iters; *iters gets the
+ * number of iterations.  Results equal those of cospdnn_engine_run. */
+int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, int max_iters,
+                                  float *layer_ms, int *iters);
+
+/* ------------------------------------------------------------------------
+ * Synthetic Graph-Challenge-style input rows, generated on the GPU: row r
+ * (global index row0 + r) of network `net` has density
+ * d = dlo + (dhi-dlo)*u and element j = (u_j < d), from SplitMix64 streams
+ * keyed by (seed, net, row).  format COSPDNN_INPUT_U8 writes [rows][neuron]
+ * bytes, COSPDNN_INPUT_BITS [rows][neuron/8] packed bits.  Asynchronous.
+ */
+int cospdnn_synth_input(void *out, int64_t rows, int neuron, uint64_t seed, int net, int64_t row0,
+                        double dlo, double dhi, int format, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

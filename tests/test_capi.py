@@ -1,0 +1,48 @@
+"""The C-ABI library loads and exports every function include/*.h declares
+(no compute calls: this runs without a GPU)."""
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(cospdnn_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ("cospdnn_layer", "cospdnn_prune_compact", "cospdnn_engine_run"):
+        assert n in names
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_library_exports(name):
+    import cospdnn_b200
+    L = cospdnn_b200.lib()
+    assert hasattr(L, name), f"{name} declared in include/ but not exported"
+
+
+def test_version_and_error_string():
+    import cospdnn_b200
+    L = cospdnn_b200.lib()
+    assert L.cospdnn_version() >= 100
+    assert isinstance(L.cospdnn_last_error(), bytes)
+
+
+def test_invalid_arguments_fail_cleanly_without_gpu():
+    import cospdnn_b200 as cs
+    L = cs.lib()
+    rc = L.cospdnn_layer(None, None, None, None, None, None, 0.0, 0, 0, 16, 16, 0, 0, None)
+    assert rc == cs.ERR_INVALID
+    assert b"null" in L.cospdnn_last_error()
+    assert L.cospdnn_prune_workspace_bytes(1000) >= 4000

@@ -1,0 +1,129 @@
+"""Parity of the whole-network engine with the FP64 oracle (GPU)."""
+import numpy as np
+import pytest
+
+from netgen import make_net, oracle_run
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def cs():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import cospdnn_b200
+    cospdnn_b200.lib()
+    return cospdnn_b200
+
+
+def run_engine(cs, nets, precision, kernel=0, tau=1e-5, runs=1):
+    """nets: list of (csc, y0, bias).  Returns per-net result dicts."""
+    eng = cs.Engine(0)
+    ids = []
+    for csc, y0, bias in nets:
+        nid = eng.add_net(y0.shape[1], len(csc), y0.shape[0], float(bias), tau, precision, kernel)
+        for l, (cp, ri, vv) in enumerate(csc):
+            eng.set_layer_csc(nid, l, cp, ri, vv)
+        ids.append(nid)
+    eng.build()
+    out = None
+    for _ in range(runs):
+        for nid, (_, y0, _) in zip(ids, nets):
+            eng.set_input(nid, y0)
+        eng.run()
+        out = [eng.result(nid) for nid in ids]
+    out_launches = eng.launch_count()
+    finals = [eng.final_values(nid, len(r["categories"])) for nid, r in zip(ids, out)]
+    eng.close()
+    for r, f in zip(out, finals):
+        r["final"] = f
+        r["launches"] = out_launches
+    return out
+
+
+def check_parity(res, ref, layers):
+    np.testing.assert_array_equal(res["alive"], ref["alive"][:layers])
+    np.testing.assert_array_equal(res["categories"], ref["categories"])
+
+
+@pytest.mark.parametrize("prec,kernel", [(0, 1), (1, 1), (2, 1)])
+def test_engine_xor_1024_matches_fp64(cs, prec, kernel):
+    csc, y0, b = make_net(1024, 12, 3000, seed=3)
+    ref = oracle_run(csc, y0, b)
+    res = run_engine(cs, [(csc, y0, b)], prec, kernel)[0]
+    check_parity(res, ref, 12)
+    assert res["launches"] > 0
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_engine_sustained_activity_matches_fp64(cs, prec):
+    """Input density U[0.25,0.45]: most rows stay alive, categories non-trivial."""
+    csc, y0, b = make_net(1024, 24, 1500, seed=5, dlo=0.25, dhi=0.45)
+    ref = oracle_run(csc, y0, b, want_final=True)
+    assert len(ref["categories"]) > 100
+    res = run_engine(cs, [(csc, y0, b)], prec, 1)[0]
+    check_parity(res, ref, 24)
+    fin_ref = ref["final"][ref["categories"]]
+    tol = {0: 1e-3, 1: 0.25, 2: 2.0}[prec]
+    assert np.abs(res["final"] - fin_ref).max() <= tol
+
+
+def test_engine_multi_network_uneven(cs):
+    nets = [make_net(1024, 10, 2500, seed=7, net=0),
+            make_net(2048, 6, 700, seed=7, net=1, dlo=0.25, dhi=0.45),
+            make_net(1024, 15, 1200, seed=7, net=2, dlo=0.2, dhi=0.4)]
+    refs = [oracle_run(*n) for n in nets]
+    res = run_engine(cs, nets, 1, 1)
+    for r, f, n in zip(res, refs, nets):
+        check_parity(r, f, len(n[0]))
+
+
+def test_engine_repeat_runs_identical(cs):
+    csc, y0, b = make_net(1024, 8, 1000, seed=9, dlo=0.2, dhi=0.4)
+    ref = oracle_run(csc, y0, b)
+    res = run_engine(cs, [(csc, y0, b)], 1, 1, runs=3)[0]
+    check_parity(res, ref, 8)
+
+
+def test_engine_zero_threshold_rule(cs):
+    csc, y0, b = make_net(1024, 10, 2000, seed=11)
+    ref = oracle_run(csc, y0, b, tau=0.0)
+    res = run_engine(cs, [(csc, y0, b)], 0, 1, tau=0.0)[0]
+    check_parity(res, ref, 10)
+
+
+def test_engine_bcsc_input_with_fuse(cs):
+    """Weights given as the reference's greedy BCSC plus a fuse permutation."""
+    from oracle import pyoracle as po
+    n, L, rows = 512, 6, 800
+    csc, y0, b = make_net(n, L, rows, seed=13, dlo=0.2, dhi=0.4)
+    rng = np.random.default_rng(0)
+    eng = cs.Engine(0)
+    nid = eng.add_net(n, L, rows, float(b), 1e-5, 0, 1)
+    folded = []
+    for l, (cp, ri, vv) in enumerate(csc):
+        fuse = rng.permutation(n).astype(np.int32)
+        row, col, val = po.csc_to_coo(cp, ri, vv)
+        bcp, bri, _, bvals = po.bcsc_greedy(row, col, val, 16)
+        eng.set_layer_bcsc(nid, l, bcp, bri, bvals, 16, fuse)
+        # the same layer with the fuse folded in, as the oracle sees it
+        bs = 16
+        V = bvals.reshape(-1, bs, bs)
+        rr, cc, ww = [], [], []
+        for bid in range(len(bcp) - 1):
+            for blk in range(bcp[bid], bcp[bid + 1]):
+                co, ro = np.nonzero(V[blk])
+                rr += list(fuse[bri[blk] + ro])
+                cc += list(bid * bs + co)
+                ww += list(V[blk][co, ro])
+        folded.append(po.coo_to_csc(np.array(rr, np.int32), np.array(cc, np.int32),
+                                    np.array(ww, np.float32), n))
+    eng.build()
+    eng.set_input(nid, y0)
+    eng.run()
+    res = eng.result(nid)
+    eng.close()
+    ref = oracle_run(folded, y0, b)
+    check_parity(res, ref, L)

@@ -1,0 +1,76 @@
+"""Per-layer survivor counts of the reference's own host loop
+(test_graph_challenge_tc, src/cospdnn.cu:172-307, built from its sources into
+oracle/_ref) against the FP64 oracle and the engine, on reference-compatible
+weights (two aligned dense 16x16 blocks per block column), where the
+reference computes the true recurrence."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from netgen import make_net, oracle_run
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libref_cospdnn.so")
+
+
+def run_reference_loop(oracle, csc, y0, bias):
+    ref = C.CDLL(REF_SO)
+    L, n = len(csc), y0.shape[1]
+    vals, rows, ptrs = [], [], []
+    for cp, ri, vv in csc:
+        row, col, val = oracle.csc_to_coo(cp, ri, vv)
+        bcp, bri, _, bvals = oracle.bcsc_greedy(row, col, val, 16)
+        vals.append(np.ascontiguousarray(bvals, np.float32))
+        rows.append(np.ascontiguousarray(bri, np.int32))
+        ptrs.append(np.ascontiguousarray(bcp, np.int32))
+    fp = C.POINTER(C.c_float)
+    ip = C.POINTER(C.c_int)
+    V = (fp * L)(*[v.ctypes.data_as(fp) for v in vals])
+    RI = (ip * L)(*[r.ctypes.data_as(ip) for r in rows])
+    P = (ip * L)(*[p.ctypes.data_as(ip) for p in ptrs])
+    nv = np.array([len(v) for v in vals], np.int64)
+    nr = np.array([len(r) for r in rows], np.int64)
+    npp = np.array([len(p) for p in ptrs], np.int64)
+    feats = np.full(64, -1, np.int32)
+    kms, wms = C.c_double(), C.c_double()
+    last = C.c_int()
+    tail = C.create_string_buffer(4096)
+    ref.ref_run_network.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_int, C.c_char_p, C.c_int]
+    y = np.ascontiguousarray(y0, np.uint8)
+    rc = ref.ref_run_network(y.ctypes.data, y.shape[0], n, L, C.addressof(V), nv.ctypes.data,
+                             C.addressof(RI), nr.ctypes.data, C.addressof(P), npp.ctypes.data,
+                             float(bias), C.addressof(kms), C.addressof(wms), C.addressof(last),
+                             feats.ctypes.data, 64, tail, 4096)
+    assert rc == 0, tail.value.decode()
+    return feats, kms.value
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference not built (make -C oracle ref)")
+def test_reference_loop_counts_match_oracle_and_engine(oracle):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import cospdnn_b200 as cs
+    n, L, rows = 1024, 16, 2048
+    csc, y0, b = make_net(n, L, rows, seed=31, kind="r1", dlo=0.1, dhi=0.3)
+    feats, kms = run_reference_loop(oracle, csc, y0, b)
+    ref = oracle_run(csc, y0, b)
+    # the reference prints counts for the layers it compacts (l <= 21)
+    np.testing.assert_array_equal(feats[:L], ref["alive"])
+    eng = cs.Engine(0)
+    nid = eng.add_net(n, L, rows, float(b), 1e-5, cs.PREC_FP16, cs.KERNEL_AUTO)
+    for l, (cp, ri, vv) in enumerate(csc):
+        eng.set_layer_csc(nid, l, cp, ri, vv)
+    eng.build()
+    eng.set_input(nid, y0)
+    eng.run()
+    res = eng.result(nid)
+    eng.close()
+    np.testing.assert_array_equal(res["alive"], ref["alive"])
+    assert kms > 0
