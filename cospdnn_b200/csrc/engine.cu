@@ -121,6 +121,7 @@ struct cospdnn_engine {
     unsigned long long *launches = nullptr;
     unsigned int *finished = nullptr;
     int *loop_guard = nullptr;
+    int *abort_flag = nullptr;  // raised by a layer kernel whose bounded wait expired
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle loop{};
@@ -202,7 +203,7 @@ int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std
     k0.fn = (void *)k_init_run;
     k0.grid = dim3(sms * 4);
     k0.block = dim3(256);
-    k0.arg(nets).arg(nn).arg(launches).arg(guard);
+    k0.arg(nets).arg(nn).arg(launches).arg(guard).arg(e->abort_flag);
     for (int prec : plain_precs) {
         KSpec k;
         k.fn = prec == COSPDNN_PREC_FP32 ? (void *)k_layer_plain<float>
@@ -217,7 +218,7 @@ int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std
     }
     for (int prec : tc_precs) {
         KSpec k;
-        int rc = tc_layer_spec(k, nets, nn, prec, launches, sms);
+        int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, sms);
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
@@ -237,7 +238,7 @@ int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std
         k4.grid = dim3(nn);
         k4.block = dim3(kCompactThreads);
         k4.arg(nets).arg(nn).arg(e->finished).arg(e->loop).arg(use_cond).arg(guard)
-            .arg(e->max_layers + 2).arg(launches);
+            .arg(e->max_layers + 2).arg((const int *)e->abort_flag).arg(launches);
     }
     return COSPDNN_OK;
 }
@@ -486,8 +487,10 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     e->launches = dalloc<unsigned long long>(1, e->owned);
     e->finished = dalloc<unsigned int>(1, e->owned);
     e->loop_guard = dalloc<int>(1, e->owned);
-    CSP_CHECK(e->scratch && e->launches && e->finished && e->loop_guard, COSPDNN_ERR_NOMEM,
+    e->abort_flag = dalloc<int>(1, e->owned);
+    CSP_CHECK(e->scratch && e->launches && e->finished && e->loop_guard && e->abort_flag, COSPDNN_ERR_NOMEM,
               "build: allocation failed");
+    CSP_CUDA(cudaMemset(e->abort_flag, 0, sizeof(int)));
     CSP_CUDA(cudaMemset(e->finished, 0, sizeof(unsigned int)));
     CSP_CUDA(cudaMemset(e->launches, 0, sizeof(unsigned long long)));
     int rc = build_graph(e, plain, tc);

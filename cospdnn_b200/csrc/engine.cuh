@@ -83,6 +83,11 @@ struct NetDev {
 
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
 
+// Counts kernel launches of a run (one atomic per launch, block 0 thread 0).
+__device__ __forceinline__ void count_launch(unsigned long long *launches) {
+    if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
+}
+
 // Bound on |z_fast - z_FP64| for one row of layer `lw` (z = pre-activation).
 //   e_in  bound on the row's input error, m_in max |input| (fast values)
 //   steps number of roundings in the fast accumulation of one output

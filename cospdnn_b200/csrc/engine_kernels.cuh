@@ -8,16 +8,13 @@
 
 namespace cospdnn {
 
-__device__ __forceinline__ void count_launch(unsigned long long *launches) {
-    if (launches && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(launches, 1ull);
-}
-
 // ---- K0: start of a run --------------------------------------------------
 __global__ void k_init_run(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches,
-                           int *loop_guard) {
+                           int *loop_guard, int *abort_flag) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (launches) *launches = 1ull;
         *loop_guard = 0;
+        *abort_flag = 0;
     }
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
@@ -273,7 +270,7 @@ constexpr int kCompactThreads = 1024;
 __global__ void __launch_bounds__(kCompactThreads)
     k_compact(const NetDev *__restrict__ nets, int nnets, unsigned int *finished_ctas,
               cudaGraphConditionalHandle loop, int use_cond, int *loop_guard, int max_iters,
-              unsigned long long *launches) {
+              const int *abort_flag, unsigned long long *launches) {
     count_launch(launches);
     __shared__ int warp_tot[kCompactThreads / 32];
     __shared__ int carry, s_done, s_layer, s_R;
@@ -340,7 +337,7 @@ __global__ void __launch_bounds__(kCompactThreads)
             int live = 0;
             for (int i = 0; i < nnets; ++i) live |= !(*(volatile int *)&nets[i].st->done);
             const int it = ++*loop_guard;
-            if (it > max_iters) {
+            if (it > max_iters || *(volatile const int *)abort_flag) {
                 for (int i = 0; i < nnets; ++i) nets[i].st->err = COSPDNN_ERR_DEVICE;
                 live = 0;
             }

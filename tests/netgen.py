@@ -28,3 +28,51 @@ def oracle_run(csc, y0, bias, tau=1e-5, want_final=False):
     alive = po.survivors_per_layer(res["death"], L)
     cats = np.nonzero(res["death"] == L)[0].astype(np.int32)
     return dict(alive=alive, categories=cats, death=res["death"], final=res["final"])
+
+
+def half_block_layer(neuron, seed, net, layer, val=0.125):
+    """Reference-kernel-friendly layer: output block column g (outputs
+    16g..16g+7) reads the first 8 rows of two aligned input blocks
+    g^a and g^b (a != b per layer), value `val`; outputs 16g+8..16g+15 have no
+    inputs.  The reference kernel's last pipeline stage (second half of the
+    second block) then carries only zero weights, so its race cannot change
+    the result, and the all-equal 8x8 quadrants are symmetric."""
+    nb = neuron // 16
+    g = SplitMix(seed * 1000003 + net * 1009 + layer)
+    a = g.next() % nb
+    b = g.next() % nb
+    while b == a:
+        b = g.next() % nb
+    cols, rows = [], []
+    for blk in range(nb):
+        src = sorted([blk ^ a, blk ^ b])
+        for r in range(8):
+            ins = [16 * src[0] + k for k in range(8)] + [16 * src[1] + k for k in range(8)]
+            cols.append((16 * blk + r, ins))
+    colptr = np.zeros(neuron + 1, np.int32)
+    rowidx, vals = [], []
+    per = {c: ins for c, ins in cols}
+    for j in range(neuron):
+        ins = per.get(j, [])
+        rowidx += ins
+        vals += [val] * len(ins)
+        colptr[j + 1] = colptr[j] + len(ins)
+    return colptr, np.array(rowidx, np.int32), np.array(vals, np.float32)
+
+
+class SplitMix:
+    def __init__(self, s):
+        self.s = s & ((1 << 64) - 1)
+
+    def next(self):
+        self.s = (self.s + 0x9E3779B97F4A7C15) & ((1 << 64) - 1)
+        z = self.s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & ((1 << 64) - 1)
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & ((1 << 64) - 1)
+        return z ^ (z >> 31)
+
+
+def make_half_block_net(neuron, layers, rows, seed=1, dlo=0.1, dhi=0.3, bias=-0.3):
+    csc = [half_block_layer(neuron, seed, 0, l) for l in range(layers)]
+    y0 = po.input_binary(seed, 0, rows, neuron, dlo, dhi)
+    return csc, y0, np.float32(bias)

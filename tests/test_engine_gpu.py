@@ -48,7 +48,7 @@ def check_parity(res, ref, layers):
     np.testing.assert_array_equal(res["categories"], ref["categories"])
 
 
-@pytest.mark.parametrize("prec,kernel", [(0, 1), (1, 1), (2, 1)])
+@pytest.mark.parametrize("prec,kernel", [(0, 1), (1, 1), (2, 1), (1, 2), (2, 2)])
 def test_engine_xor_1024_matches_fp64(cs, prec, kernel):
     csc, y0, b = make_net(1024, 12, 3000, seed=3)
     ref = oracle_run(csc, y0, b)
@@ -57,25 +57,26 @@ def test_engine_xor_1024_matches_fp64(cs, prec, kernel):
     assert res["launches"] > 0
 
 
-@pytest.mark.parametrize("prec", [0, 1, 2])
-def test_engine_sustained_activity_matches_fp64(cs, prec):
+@pytest.mark.parametrize("prec,kernel", [(0, 1), (1, 1), (2, 1), (1, 2), (2, 2)])
+def test_engine_sustained_activity_matches_fp64(cs, prec, kernel):
     """Input density U[0.25,0.45]: most rows stay alive, categories non-trivial."""
     csc, y0, b = make_net(1024, 24, 1500, seed=5, dlo=0.25, dhi=0.45)
     ref = oracle_run(csc, y0, b, want_final=True)
     assert len(ref["categories"]) > 100
-    res = run_engine(cs, [(csc, y0, b)], prec, 1)[0]
+    res = run_engine(cs, [(csc, y0, b)], prec, kernel)[0]
     check_parity(res, ref, 24)
     fin_ref = ref["final"][ref["categories"]]
     tol = {0: 1e-3, 1: 0.25, 2: 2.0}[prec]
     assert np.abs(res["final"] - fin_ref).max() <= tol
 
 
-def test_engine_multi_network_uneven(cs):
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_engine_multi_network_uneven(cs, kernel):
     nets = [make_net(1024, 10, 2500, seed=7, net=0),
             make_net(2048, 6, 700, seed=7, net=1, dlo=0.25, dhi=0.45),
             make_net(1024, 15, 1200, seed=7, net=2, dlo=0.2, dhi=0.4)]
     refs = [oracle_run(*n) for n in nets]
-    res = run_engine(cs, nets, 1, 1)
+    res = run_engine(cs, nets, 1, kernel)
     for r, f, n in zip(res, refs, nets):
         check_parity(r, f, len(n[0]))
 
@@ -127,3 +128,22 @@ def test_engine_bcsc_input_with_fuse(cs):
     eng.close()
     ref = oracle_run(folded, y0, b)
     check_parity(res, ref, L)
+
+
+@pytest.mark.parametrize("n,rows", [(4096, 700), (512, 130), (256, 1)])
+def test_engine_tcgen05_shapes(cs, n, rows):
+    """Ragged row tiles (rows not a multiple of 128), narrow and wide layers."""
+    csc, y0, b = make_net(n, 6, rows, seed=17, dlo=0.2, dhi=0.45, bias=-0.3)
+    ref = oracle_run(csc, y0, b, want_final=True)
+    res = run_engine(cs, [(csc, y0, b)], 1, 2)[0]
+    check_parity(res, ref, 6)
+
+
+def test_engine_tcgen05_layer_values_match_cuda_core(cs):
+    """Same net, same FP16 storage: the tcgen05 and CUDA-core kernels produce
+    final activations within the FP16 rounding of each other."""
+    csc, y0, b = make_net(1024, 8, 600, seed=19, dlo=0.25, dhi=0.45)
+    r_tc = run_engine(cs, [(csc, y0, b)], 1, 2)[0]
+    r_cc = run_engine(cs, [(csc, y0, b)], 1, 1)[0]
+    np.testing.assert_array_equal(r_tc["categories"], r_cc["categories"])
+    assert np.abs(r_tc["final"] - r_cc["final"]).max() <= 0.125
