@@ -223,9 +223,12 @@ def main():
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 CUDA cores, 2 tcgen05")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rows", type=int, default=None, help="override the rows per network (profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     nets, prec, dens = config_nets(args.config)
+    if args.rows:
+        nets = [(n, l, args.rows) for n, l, _ in nets]
     if args.precision:
         prec = args.precision
     if args.impl == "reference":
