@@ -16,7 +16,7 @@ namespace {
 
 // ---- input conversion: any format -> compute type, per-row error and max --
 template <typename T, int FMT>
-__global__ void k_convert_input(const void *__restrict__ src, int rows, int N, T *__restrict__ y0,
+__global__ void k_convert_input(const void *__restrict__ src, int rows, int N, int tiled, T *__restrict__ y0,
                                 float *__restrict__ y0_f32, float *__restrict__ err0,
                                 float *__restrict__ mx0) {
     // one warp per row
@@ -31,7 +31,7 @@ __global__ void k_convert_input(const void *__restrict__ src, int rows, int N, T
             else if (FMT == COSPDNN_INPUT_F32) x = ((const float *)src)[r * N + j];
             else x = (float)((((const uint8_t *)src)[r * (N / 8) + (j >> 3)] >> (j & 7)) & 1u);
             const T v = act_traits<T>::from_f(x);
-            y0[r * N + j] = v;
+            y0[act_index(tiled, N, r, j)] = v;
             if (y0_f32) y0_f32[r * N + j] = x;
             e = fmaxf(e, fabsf(act_traits<T>::to_f(v) - x));
             m = fmaxf(m, fabsf(x));
@@ -49,12 +49,12 @@ __global__ void k_convert_input(const void *__restrict__ src, int rows, int N, T
 template <typename T>
 __global__ void k_gather_final(const NetDev *__restrict__ nd_p, float *__restrict__ out, int64_t max_rows) {
     const NetDev &nd = *nd_p;
-    const int R = nd.st->R, par = nd.st->layer & 1, N = nd.N;
-    const T *act = (const T *)nd.act[par];
+    const int R = nd.st->R, N = nd.N;
+    const T *act = (const T *)nd.act[nd.st->in_buf];
     const int64_t total = (int64_t)min((int64_t)R, max_rows) * N;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t q = i / N, j = i % N;
-        out[i] = act_traits<T>::to_f(act[(int64_t)nd.pos[par][q] * N + j]);
+        out[i] = act_traits<T>::to_f(act[act_index(nd.tiled, N, q, (int)j)]);
     }
 }
 
@@ -125,7 +125,7 @@ struct cospdnn_engine {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle loop{};
-    KSpec k0, k2, k3, k4_graph, k4_eager;
+    KSpec k0, k2, k3, k4_graph, k4_eager, k5;
     std::vector<KSpec> layer_specs;
     std::vector<long long *> packbuf;  // per net: device buffer for result_async
     ~cospdnn_engine() {
@@ -231,7 +231,14 @@ int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std
     k3.fn = (void *)k_replay;
     k3.grid = dim3(e->replay_ctas);
     k3.block = dim3(kReplayThreads);
+    k3.smem = sizeof(double) * 2 * (size_t)std::min(e->max_n, kReplaySmemN);
+    CSP_CUDA(cudaFuncSetAttribute(k3.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k3.smem));
     k3.arg(nets).arg(nn).arg(e->scratch).arg(e->max_n).arg(launches);
+    KSpec &k5 = e->k5;
+    k5.fn = (void *)k_copy_rows;
+    k5.grid = dim3(sms * 8);
+    k5.block = dim3(256);
+    k5.arg(nets).arg(nn).arg(launches);
     for (int use_cond = 0; use_cond < 2; ++use_cond) {
         KSpec &k4 = use_cond ? e->k4_graph : e->k4_eager;
         k4.fn = (void *)k_compact;
@@ -278,10 +285,11 @@ int build_graph(cospdnn_engine *e, const std::vector<int> &plain_precs, const st
     std::vector<cudaGraphNode_t> layer_nodes(e->layer_specs.size());
     for (size_t i = 0; i < e->layer_specs.size(); ++i)
         if ((rc = add_node(body, &layer_nodes[i], nullptr, 0, e->layer_specs[i]))) return rc;
-    cudaGraphNode_t k2, k3, k4;
+    cudaGraphNode_t k2, k3, k4, k5;
     if ((rc = add_node(body, &k2, layer_nodes.data(), (int)layer_nodes.size(), e->k2))) return rc;
     if ((rc = add_node(body, &k3, &k2, 1, e->k3))) return rc;
     if ((rc = add_node(body, &k4, &k3, 1, e->k4_graph))) return rc;
+    if ((rc = add_node(body, &k5, &k4, 1, e->k5))) return rc;
     CSP_CUDA(cudaGraphInstantiate(&e->exec, e->graph, 0));
     return COSPDNN_OK;
 }
@@ -313,6 +321,7 @@ extern "C" int cospdnn_engine_add_net(cospdnn_engine *e, const cospdnn_net_desc 
     CSP_CHECK(e && d, COSPDNN_ERR_INVALID, "add_net: null argument");
     CSP_CHECK(!e->built, COSPDNN_ERR_STATE, "add_net: engine already built");
     CSP_CHECK(d->neuron > 0 && d->layers > 0 && d->rows >= 0, COSPDNN_ERR_INVALID, "add_net: bad sizes");
+    CSP_CHECK(d->neuron % 8 == 0, COSPDNN_ERR_UNSUPPORTED, "add_net: neuron must be a multiple of 8");
     CSP_CHECK(d->precision >= 0 && d->precision <= 2, COSPDNN_ERR_INVALID, "add_net: bad precision");
     CSP_CHECK(d->kernel >= 0 && d->kernel <= 2, COSPDNN_ERR_INVALID, "add_net: bad kernel");
     CSP_CHECK(!(d->kernel == COSPDNN_KERNEL_TCGEN05 && d->precision == COSPDNN_PREC_FP32),
@@ -443,15 +452,17 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         d.bias = n.d.bias;
         d.tau = n.d.threshold;
         d.layers = n.d_layers;
-        const size_t es = elem_size(d.prec), act = (size_t)R * N * es;
+        d.tiled = d.kernel == COSPDNN_KERNEL_TCGEN05;
+        const size_t rows_pad = (size_t)(R + 127) / 128 * 128;
+        const size_t es = elem_size(d.prec), act = rows_pad * N * es;
         d.y0 = dalloc<char>(act, e->owned);
         d.act[0] = dalloc<char>(act, e->owned);
         d.act[1] = dalloc<char>(act, e->owned);
         float *err0 = dalloc<float>(R, e->owned), *mx0 = dalloc<float>(R, e->owned);
         d.err0 = err0;
         d.mx0 = mx0;
+        d.cmap = dalloc<int32_t>(R, e->owned);
         for (int b = 0; b < 2; ++b) {
-            d.pos[b] = dalloc<int32_t>(R, e->owned);
             d.orig[b] = dalloc<int32_t>(R, e->owned);
             d.err[b] = dalloc<float>(R, e->owned);
             d.mx[b] = dalloc<float>(R, e->owned);
@@ -462,11 +473,13 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         d.alive_count = dalloc<long long>(d.L, e->owned);
         d.recheck_count = dalloc<long long>(d.L, e->owned);
         d.st = dalloc<NetState>(1, e->owned);
-        CSP_CHECK(d.y0 && d.act[0] && d.act[1] && err0 && mx0 && d.pos[0] && d.pos[1] && d.orig[0] &&
+        CSP_CHECK(d.y0 && d.act[0] && d.act[1] && err0 && mx0 && d.cmap && d.orig[0] &&
                       d.orig[1] && d.err[0] && d.err[1] && d.mx[0] && d.mx[1] && d.stat && d.cls &&
                       d.ulist && d.alive_count && d.recheck_count && d.st,
                   COSPDNN_ERR_NOMEM, "build: device allocation failed");
         CSP_CUDA(cudaMemset((void *)d.y0, 0, act));
+        CSP_CUDA(cudaMemset(d.act[0], 0, act));
+        CSP_CUDA(cudaMemset(d.act[1], 0, act));
         CSP_CUDA(cudaMemset(err0, 0, sizeof(float) * R));
         CSP_CUDA(cudaMemset(mx0, 0, sizeof(float) * R));
         CSP_CUDA(cudaMemset(d.st, 0, sizeof(NetState)));
@@ -545,9 +558,9 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
 #define CSP_CONV(T)                                                                                      \
     do {                                                                                                 \
         T *dst = (T *)n.dev.y0;                                                                          \
-        if (format == COSPDNN_INPUT_U8) k_convert_input<T, COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, R, N, dst, f32, err0, mx0); \
-        else if (format == COSPDNN_INPUT_F32) k_convert_input<T, COSPDNN_INPUT_F32><<<blocks, 256, 0, s>>>(src, R, N, dst, f32, err0, mx0); \
-        else k_convert_input<T, COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, R, N, dst, f32, err0, mx0); \
+        if (format == COSPDNN_INPUT_U8) k_convert_input<T, COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, R, N, n.dev.tiled, dst, f32, err0, mx0); \
+        else if (format == COSPDNN_INPUT_F32) k_convert_input<T, COSPDNN_INPUT_F32><<<blocks, 256, 0, s>>>(src, R, N, n.dev.tiled, dst, f32, err0, mx0); \
+        else k_convert_input<T, COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, R, N, n.dev.tiled, dst, f32, err0, mx0); \
     } while (0)
     if (n.d.precision == COSPDNN_PREC_FP32) CSP_CONV(float);
     else if (n.d.precision == COSPDNN_PREC_FP16) CSP_CONV(__half);
@@ -676,6 +689,7 @@ extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, in
         if (!rc) rc = launch(e->k2, s);
         if (!rc) rc = launch(e->k3, s);
         if (!rc) rc = launch(e->k4_eager, s);
+        if (!rc) rc = launch(e->k5, s);
         if (rc) break;
         err = cudaEventSynchronize(b);
         if (err != cudaSuccess) { rc = cuda_fail(err, "profile_layers: event"); break; }

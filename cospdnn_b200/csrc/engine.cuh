@@ -38,25 +38,39 @@ struct LayerDev {
     const int32_t *ell_idx;
     const float *ell_val;
     int K;
-    // 16x16 aligned block view (tcgen05 kernel): output block column c has
-    // blocks blk_ptr[c]..blk_ptr[c+1]; blk_row[b] is the input block (rows
-    // 16*blk_row .. +16); blk_b holds each block as the MMA B operand
-    // (16 outputs x 16 inputs, K-major, 512 bytes per block).
-    const int32_t *blk_ptr;
-    const int32_t *blk_row;
-    const void *blk_b;
-    int max_blocks;  // max blocks in one output block column
+    // tcgen05 schedule (16x16 aligned blocks of W, built by tc_build_blocks):
+    // output block columns are taken in chunks of up to 32 (one TMEM
+    // accumulator of 16 columns each); within a chunk the MMAs are ordered by
+    // input block and split into stages, each stage = one contiguous run of
+    // input blocks (a_count <= 8, one bulk copy of the A tiles) + its MMAs'
+    // B operands (contiguous in tc_b, one bulk copy).
+    //   tc_chunk_ptr[h]..[h+1]  stages of chunk h
+    //   tc_stage[s]             {a_first, a_count, b_first, n_mma}
+    //   tc_code[b]              MMA b: bits 0-2 A block within the run,
+    //                           bits 3-7 accumulator (column within the chunk),
+    //                           bit 8 first MMA into that accumulator
+    //   tc_b                    B operands, 512 bytes each, in stage order
+    //   tc_used[h]              bit j: column j of chunk h has any weight
+    const int32_t *tc_chunk_ptr;
+    const int4 *tc_stage;
+    const uint16_t *tc_code;
+    const void *tc_b;
+    const uint32_t *tc_used;
+    int tc_nchunks;
+    int max_blocks;  // max 16x16 blocks in one output block column (error bound)
     float S;         // max_j sum_i |W_ij|
     float dW;        // max_j sum_i |W'_ij - W_ij|, W' = weights in the compute type
 };
 
 struct NetState {
-    int layer;  // next layer to compute
-    int R;      // rows entering `layer`
-    int done;   // finished (all rows pruned or all layers computed)
-    int nunc;   // rows of this layer whose keep/prune decision needs the FP64 replay
-    int err;    // device-side error code (0 = ok)
-    int pad[3];
+    int layer;   // next layer to compute
+    int R;       // rows entering `layer` (rows 0..R-1 of its input buffer)
+    int done;    // finished (all rows pruned or all layers computed)
+    int nunc;    // rows of this layer whose keep/prune decision needs the FP64 replay
+    int err;     // device-side error code (0 = ok)
+    int in_buf;  // act[in_buf] is the input of `layer` (layer 0 reads y0)
+    int copy_R;  // rows the pending compaction copies (0 = none pending)
+    int pad;
 };
 
 struct NetDev {
@@ -68,8 +82,9 @@ struct NetDev {
     const float *y0_f32;     // exact input when the compute type cannot hold it (else NULL)
     const float *err0;       // [rows] bound on |y0(compute) - y0(exact)|
     const float *mx0;        // [rows] max |y0|
-    void *act[2];            // [rows][N] ping-pong activations
-    int32_t *pos[2];         // list: row position in the layer's input buffer
+    int tiled;               // activation layout: 0 row-major, 1 MMA tiles (see act_index)
+    void *act[2];            // ping-pong activations, rows padded to a multiple of 128
+    int32_t *cmap;           // [rows] compaction map: new row q <- output row cmap[q]
     int32_t *orig[2];        // list: original row id
     float *err[2];           // list: bound on |Y(fast) - Y(FP64)| of the row's inputs
     float *mx[2];            // list: max |Y(fast)| of the row's inputs
@@ -82,6 +97,20 @@ struct NetDev {
 };
 
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
+
+// Element index of (row, feature) in an activation buffer of width N.
+// Row-major: row*N + f.  MMA tiles (tcgen05 nets): rows in tiles of 128 and
+// features in blocks of 16; each (tile, block) is a contiguous 4 KB operand in
+// the canonical K-major core-matrix order of tcgen05 (8 rows x 16 bytes per
+// core matrix, the two 8-feature halves 128 bytes apart, 8-row groups 256
+// bytes apart), so one bulk copy brings a whole MMA A operand into shared
+// memory and the epilogue writes one output block as one such operand.
+__host__ __device__ __forceinline__ int64_t act_index(int tiled, int N, int64_t row, int f) {
+    if (!tiled) return row * N + f;
+    const int64_t tile = row >> 7;
+    const int m = (int)(row & 127), fb = f >> 4, k = f & 15;
+    return (tile * (N >> 4) + fb) * 2048 + (m >> 3) * 128 + (k >> 3) * 64 + (m & 7) * 8 + (k & 7);
+}
 
 // Counts kernel launches of a run (one atomic per launch, block 0 thread 0).
 __device__ __forceinline__ void count_launch(unsigned long long *launches) {

@@ -1,7 +1,16 @@
 // Kernels of the device-driven layer loop.  Every kernel reads the per-net
-// state (current layer, active rows) from device memory, so one captured graph
-// serves every layer and every network; grids are fixed and loop over the
-// work that the state describes.
+// state (current layer, active rows, buffer roles) from device memory, so one
+// captured graph serves every layer and every network; grids are fixed and
+// loop over the work that the state describes.
+//
+// Per iteration (every live network advances one layer):
+//   layer kernel(s)  rows 0..R-1 of IN -> OUT, per-row statistics
+//   k_classify       keep / prune / uncertain from the statistics and the
+//                    row's error bound
+//   k_replay         exact FP64 replay of the uncertain rows
+//   k_compact        stable compaction of the kept rows: new lists, state
+//   k_copy_rows      kept rows of OUT -> rows 0..R'-1 of the next input
+// IN = y0 for layer 0, else act[in_buf]; OUT = act[in_buf ^ 1].
 #pragma once
 
 #include "engine.cuh"
@@ -26,13 +35,14 @@ __global__ void k_init_run(const NetDev *__restrict__ nets, int nnets, unsigned 
             nd.st->done = (nd.rows == 0 || nd.L == 0);
             nd.st->nunc = 0;
             nd.st->err = 0;
+            nd.st->in_buf = 0;
+            nd.st->copy_R = 0;
         }
         for (int64_t l = tid; l < nd.L; l += nth) {
             nd.alive_count[l] = 0;
             nd.recheck_count[l] = 0;
         }
         for (int64_t p = tid; p < nd.rows; p += nth) {
-            nd.pos[0][p] = (int32_t)p;
             nd.orig[0][p] = (int32_t)p;
             nd.err[0][p] = nd.err0[p];
             nd.mx[0][p] = nd.mx0[p];
@@ -58,7 +68,6 @@ __global__ void __launch_bounds__(kPlainThreads)
     const int lane = threadIdx.x & 31;
     const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // units of kPlainRows rows, enumerated net after net
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
@@ -76,10 +85,10 @@ __global__ void __launch_bounds__(kPlainThreads)
             u -= cnt;
         }
         const NetDev &nd = nets[n];
-        const int N = nd.N, l = nd.st->layer, R = nd.st->R, par = l & 1;
+        const int N = nd.N, l = nd.st->layer, R = nd.st->R, par = l & 1, ib = nd.st->in_buf;
         const LayerDev lw = nd.layers[l];
-        const T *in = (const T *)(l == 0 ? nd.y0 : nd.act[par]);
-        T *out = (T *)nd.act[par ^ 1];
+        const T *in = (const T *)(l == 0 ? nd.y0 : nd.act[ib]);
+        T *out = (T *)nd.act[ib ^ 1];
         const double steps = fast_steps(nd, lw);
         const T *inrow[kPlainRows];
         T *outrow[kPlainRows];
@@ -90,7 +99,7 @@ __global__ void __launch_bounds__(kPlainThreads)
             const int p = (int)(u * kPlainRows) + r;
             valid[r] = p < R;
             const int pp = valid[r] ? p : (int)(u * kPlainRows);
-            inrow[r] = in + (int64_t)nd.pos[par][pp] * N;
+            inrow[r] = in + (int64_t)pp * N;
             outrow[r] = out + (int64_t)pp * N;
             ez[r] = z_error_bound(nd.err[par][pp], nd.mx[par][pp], lw.S, lw.dW, nd.bias, steps);
             zmax[r] = -INFINITY;
@@ -168,8 +177,10 @@ __global__ void k_classify(const NetDev *__restrict__ nets, int nnets, unsigned 
 // the current layer in the oracle's order (for each output, ascending input
 // index, separately rounded multiply and add, bias last, clamp), decide
 // keep/prune exactly, and for kept rows overwrite the fast output with the
-// FP64 values rounded to the compute type.
-constexpr int kReplayThreads = 256;
+// FP64 values rounded to the compute type.  The row is held in shared memory
+// when two copies fit (kReplaySmemN doubles each), else in global scratch.
+constexpr int kReplayThreads = 512;
+constexpr int kReplaySmemN = 8192;
 
 __device__ __forceinline__ float block_max(float v, float *red) {
     v = warp_max(v);
@@ -188,12 +199,12 @@ __device__ __forceinline__ float block_max(float v, float *red) {
 
 template <typename T>
 __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, float *red) {
-    const int N = nd.N, l = nd.st->layer, par = l & 1;
+    const int N = nd.N, l = nd.st->layer, par = l & 1, ib = nd.st->in_buf;
     const int orow = nd.orig[par][p];
     double *y = buf0, *z = buf1;
     for (int j = threadIdx.x; j < N; j += blockDim.x)
         y[j] = nd.y0_f32 ? (double)nd.y0_f32[(int64_t)orow * N + j]
-                         : act_traits<T>::to_d(((const T *)nd.y0)[(int64_t)orow * N + j]);
+                         : act_traits<T>::to_d(((const T *)nd.y0)[act_index(nd.tiled, N, orow, j)]);
     __syncthreads();
     const double b = (double)nd.bias;
     for (int ll = 0; ll <= l; ++ll) {
@@ -201,26 +212,24 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
             double acc = 0.0;
             for (int k = 0; k < lw.K; ++k) {
-                const double yi = y[lw.ell_idx[(int64_t)k * N + j]];
-                if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)lw.ell_val[(int64_t)k * N + j], yi));
+                const double yi = y[__ldg(lw.ell_idx + (int64_t)k * N + j)];
+                if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)__ldg(lw.ell_val + (int64_t)k * N + j), yi));
             }
             z[j] = clamp32d(__dadd_rn(acc, b));
         }
         __syncthreads();
         double *t = y; y = z; z = t;
     }
-    // y holds the layer-l outputs
-    float zmax = 0.0f, emax = 0.0f, ymax = 0.0f;
+    // y holds the layer-l outputs; exact keep decision on the FP64 values
     double dmax = 0.0;
     for (int j = threadIdx.x; j < N; j += blockDim.x) dmax = fmax(dmax, y[j]);
-    // exact keep decision on the FP64 values
-    zmax = block_max(dmax > (double)nd.tau ? 1.0f : 0.0f, red);
-    const bool keep = zmax > 0.5f;
+    const bool keep = block_max(dmax > (double)nd.tau ? 1.0f : 0.0f, red) > 0.5f;
+    float emax = 0.0f, ymax = 0.0f;
     if (keep) {
-        T *out = (T *)nd.act[par ^ 1] + (int64_t)p * N;
+        T *out = (T *)nd.act[ib ^ 1];
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
             const T v = act_traits<T>::from_d(y[j]);
-            out[j] = v;
+            out[act_index(nd.tiled, N, p, j)] = v;
             const double vd = act_traits<T>::to_d(v);
             emax = fmaxf(emax, __double2float_ru(fabs(vd - y[j])));
             ymax = fmaxf(ymax, (float)vd);
@@ -243,8 +252,7 @@ __global__ void __launch_bounds__(kReplayThreads)
              unsigned long long *launches) {
     count_launch(launches);
     __shared__ float red[32];
-    double *b0 = scratch + (int64_t)blockIdx.x * 2 * max_n;
-    double *b1 = b0 + max_n;
+    extern __shared__ double ysm[];
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n)
         if (!nets[n].st->done) total += nets[n].st->nunc;
@@ -257,6 +265,14 @@ __global__ void __launch_bounds__(kReplayThreads)
             u -= nets[n].st->nunc;
         }
         const NetDev &nd = nets[n];
+        double *b0, *b1;
+        if (nd.N <= kReplaySmemN) {
+            b0 = ysm;
+            b1 = ysm + nd.N;
+        } else {
+            b0 = scratch + (int64_t)blockIdx.x * 2 * max_n;
+            b1 = b0 + max_n;
+        }
         const int p = nd.ulist[u];
         if (nd.prec == COSPDNN_PREC_FP32) replay_row<float>(nd, p, b0, b1, red);
         else if (nd.prec == COSPDNN_PREC_FP16) replay_row<__half>(nd, p, b0, b1, red);
@@ -304,7 +320,7 @@ __global__ void __launch_bounds__(kCompactThreads)
             __syncthreads();
             if (keep) {
                 const int q = carry + (wid ? warp_tot[wid - 1] : 0) + __popc(m & ((1u << lane) - 1u));
-                nd.pos[par ^ 1][q] = p;
+                nd.cmap[q] = p;
                 nd.orig[par ^ 1][q] = nd.orig[par][p];
                 nd.err[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 1]);
                 nd.mx[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 2]);
@@ -325,7 +341,16 @@ __global__ void __launch_bounds__(kCompactThreads)
             nd.st->R = carry;
             nd.st->layer = l + 1;
             nd.st->done = (carry == 0 || l + 1 >= nd.L);
+            if (carry == R) {
+                // nothing pruned: the output buffer is the next input as it is
+                nd.st->in_buf ^= 1;
+                nd.st->copy_R = 0;
+            } else {
+                nd.st->copy_R = carry;  // k_copy_rows moves the kept rows
+            }
         }
+    } else if (threadIdx.x == 0) {
+        nd.st->copy_R = 0;
     }
     // the last CTA to finish decides whether the graph loop runs again
     if (threadIdx.x == 0) {
@@ -343,6 +368,41 @@ __global__ void __launch_bounds__(kCompactThreads)
             }
             if (use_cond) cudaGraphSetConditional(loop, live ? 1u : 0u);
         }
+    }
+}
+
+// ---- K5: move the kept rows to the front of the next input buffer ---------
+// Row q of act[in_buf] <- row cmap[q] of act[in_buf ^ 1], in 16-byte pieces
+// (row-major: consecutive; MMA tiles: the two 8-feature halves of each block).
+__global__ void k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
+    count_launch(launches);
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    int64_t total = 0;
+    for (int n = 0; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        const int es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2;
+        total += (int64_t)nd.st->copy_R * (nd.N * es / 16);
+    }
+    for (int64_t i = tid; i < total; i += nth) {
+        int64_t u = i;
+        int n = 0;
+        int es = 4, pieces = 1;
+        for (; n < nnets; ++n) {
+            es = nets[n].prec == COSPDNN_PREC_FP32 ? 4 : 2;
+            pieces = nets[n].N * es / 16;
+            const int64_t cnt = (int64_t)nets[n].st->copy_R * pieces;
+            if (u < cnt) break;
+            u -= cnt;
+        }
+        const NetDev &nd = nets[n];
+        const int N = nd.N, ib = nd.st->in_buf, per = 16 / es;
+        const int q = (int)(u / pieces), f = (int)(u % pieces) * per;
+        const int p = nd.cmap[q];
+        const char *src = (const char *)nd.act[ib ^ 1];
+        char *dst = (char *)nd.act[ib];
+        const uint4 v = *reinterpret_cast<const uint4 *>(src + act_index(nd.tiled, N, p, f) * es);
+        *reinterpret_cast<uint4 *>(dst + act_index(nd.tiled, N, q, f) * es) = v;
     }
 }
 

@@ -1,27 +1,34 @@
 // tcgen05 layer kernel: FP16 / BF16 activations, FP32 accumulation in TMEM.
 //
-// Work item = (network, tile of 128 active rows, group of kGroup output block
-// columns of 16 outputs).  For every 16x16 weight block b of an output block
-// column c the kernel issues one MMA
-//     D_c[128 x 16] (+)= A[128 rows x 16 inputs of block b] * B_b[16 x 16]
-// (M=128, N=16, K=16, kind::f16).  A is gathered from the active rows of the
-// layer's input (row list = the previous layer's compaction), so pruned rows
-// are never read.  Roles (9 warps):
-//   warps 0-3  loaders: cp.async of each row's 32 bytes + the 512-byte B
-//              block into a stage of the shared-memory ring (canonical
-//              K-major, no-swizzle core-matrix layout), completion signalled
-//              by cp.async.mbarrier.arrive on the stage's `full` barrier;
-//   warp 4     MMA issuer: one thread waits `full`, issues tcgen05.mma and
-//              tcgen05.commit to the stage's `empty` barrier; after the last
-//              block of an item it commits to the item's `tfull` barrier;
-//   warps 5-8  epilogue: tcgen05.ld of the accumulators (TMEM lane = row),
-//              bias + clamp(0,32), store in the compute type, per-row
-//              statistics for the keep/prune decision (atomicMax).
-// Accumulators are double-buffered in TMEM (2 x kGroup x 16 columns) so the
-// epilogue of one item overlaps the MMAs of the next.  Every wait is bounded;
-// on timeout the CTA raises `abort`, drains its copies and MMAs, frees TMEM
-// and returns, and the engine reports COSPDNN_ERR_DEVICE.
+// W_l is cut into 16x16 aligned blocks.  Work item = (network, tile of 128
+// active rows, chunk of up to 32 output block columns); the chunk's 32
+// accumulators (128 rows x 16 outputs, FP32) fill the 512 TMEM columns.  For
+// every block b (input block i -> output block column c) one MMA
+//     D_c[128 x 16] (+)= A_i[128 rows x 16 inputs] * B_b[16 x 16]
+// (M=128, N=16, K=16, kind::f16).  The MMAs of a chunk run input-stationary:
+// ordered by input block, so each A tile is fetched once per chunk and feeds
+// every accumulator of the chunk that needs it, and consecutive MMAs write
+// different accumulators (no serialising dependence).  The host-built
+// schedule (tc_build_blocks) groups them into stages: one contiguous run of
+// up to 8 input blocks (one bulk copy of the A tiles; activations of tcgen05
+// nets are stored as MMA tiles, see act_index) plus the stage's B operands
+// and MMA codes (one bulk copy each, stored in stage order).
+// Roles (6 warps):
+//   warp 0     producer: one thread issues the stage's bulk copies
+//              (cp.async.bulk, no multicast) on the stage's `full` mbarrier;
+//   warp 1     MMA issuer: one thread waits `full`, issues the stage's
+//              tcgen05.mma and one tcgen05.commit to the stage's `empty`;
+//              after the last stage of an item it commits to `tfull`;
+//   warps 2-5  epilogue: tcgen05.ld of the accumulators (TMEM lane = row),
+//              bias + clamp(0,32), store in the compute type (32 bytes per
+//              row and output block of the output tile), per-row statistics
+//              for the keep/prune decision (atomicMax); then `tempty`.
+// While the epilogue drains TMEM the producer keeps prefetching the next
+// item's stages.  Every wait is bounded; on timeout the CTA raises `abort`,
+// drains its copies and MMAs, frees TMEM and returns, and the engine reports
+// COSPDNN_ERR_DEVICE.
 #include <algorithm>
+#include <map>
 
 #include "tc_layer.cuh"
 
@@ -29,30 +36,36 @@ namespace cospdnn {
 namespace {
 
 constexpr int kTileRows = 128;
-constexpr int kGroup = 8;                 // output block columns per work item
-constexpr int kStages = 20;  // ~92 KB of stages: at most two CTAs (2 x 256 TMEM columns) per SM
-constexpr int kStageA = kTileRows * 32;   // 128 rows x 16 inputs x 2 bytes
-constexpr int kStageB = 512;              // 16 x 16 x 2 bytes
-constexpr int kStageBytes = kStageA + kStageB;
-constexpr int kLoaderWarps = 4;
-constexpr int kMmaWarp = 4;
-constexpr int kEpiWarp0 = 5;
-constexpr int kEpiWarps = 4;
-constexpr int kThreads = (kLoaderWarps + 1 + kEpiWarps) * 32;
-constexpr int kTmemCols = 2 * kGroup * 16;  // two accumulator buffers
+constexpr int kChunk = 32;                   // output block columns per item
+constexpr int kMaxA = 8;                     // A tiles (input blocks) per stage
+constexpr int kMaxMma = 64;                  // MMAs per stage
+constexpr int kTileBytes = kTileRows * 32;   // one A tile: 128 rows x 16 inputs x 2 bytes
+constexpr int kBBytes = 512;                 // one B operand: 16 x 16 x 2 bytes
+constexpr int kStageA = kMaxA * kTileBytes;
+constexpr int kStageB = kMaxMma * kBBytes;
+constexpr int kStageCode = kMaxMma * 2;
+constexpr int kStageBytes = kStageA + kStageB + kStageCode;
+constexpr int kStages = 3;
+constexpr int kMaxGap = 1;                   // unused input blocks a stage may span
+constexpr int kProducerWarp = 0;
+constexpr int kMmaWarp = 1;
+constexpr int kEpiWarps = 4;  // warps 2..5: (warp & 3) covers the four TMEM lane quarters
+constexpr int kThreads = (2 + kEpiWarps) * 32;
+constexpr int kTmemCols = kChunk * 16;      // 512: one accumulator per chunk column
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
-struct __align__(16) TcSmem {
+struct __align__(128) TcSmem {
     uint8_t stage[kStages][kStageBytes];
     unsigned long long full[kStages];
     unsigned long long empty[kStages];
-    unsigned long long tfull[2];
-    unsigned long long tempty[2];
+    unsigned long long tfull;
+    unsigned long long tempty;
     unsigned long long fin;
     uint32_t tmem_base;
     volatile int abort;
 };
 constexpr size_t kSmemBytes = sizeof(TcSmem) + 128;
+static_assert(kSmemBytes <= 227 * 1024, "tcgen05 layer kernel shared memory");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -85,11 +98,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, uint32_t parity
 __device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes));
 }
-__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long *b) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+// Bulk copy global -> this CTA's shared memory, completing on `bar` (no multicast).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar)));
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -112,56 +127,57 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b,
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void mma_commit(unsigned long long *b) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b))
-                 : "memory");
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(b)));
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
-    uint32_t r[16];
+// 32 lanes x 32 columns (two accumulators) of TMEM into registers.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+    uint32_t r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 struct Item {
-    int net, tile, c0, c1;
+    int net, tile, chunk;
 };
 
-// Work items of this layer for tcgen05 nets of precision `prec`.
 __device__ __forceinline__ bool tc_net(const NetDev &nd, int prec) {
     return nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.prec == prec && !nd.st->done;
 }
+// Work items of this layer (tile-major, so CTAs running at the same time share
+// the row tile's A operands in L2).
 __device__ __forceinline__ int64_t tc_items(const NetDev *nets, int nnets, int prec) {
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (!tc_net(nd, prec)) continue;
-        const int nb = nd.N / 16;
-        total += (int64_t)((nd.st->R + kTileRows - 1) / kTileRows) * ((nb + kGroup - 1) / kGroup);
+        total += (int64_t)((nd.st->R + kTileRows - 1) / kTileRows) * nd.layers[nd.st->layer].tc_nchunks;
     }
     return total;
 }
 __device__ __forceinline__ Item tc_item(const NetDev *nets, int nnets, int prec, int64_t idx) {
-    Item it{0, 0, 0, 0};
+    Item it{0, 0, 0};
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (!tc_net(nd, prec)) continue;
-        const int nb = nd.N / 16, groups = (nb + kGroup - 1) / kGroup;
-        const int64_t cnt = (int64_t)((nd.st->R + kTileRows - 1) / kTileRows) * groups;
+        const int nch = nd.layers[nd.st->layer].tc_nchunks;
+        const int64_t cnt = (int64_t)((nd.st->R + kTileRows - 1) / kTileRows) * nch;
         if (idx < cnt) {
             it.net = n;
-            it.tile = (int)(idx / groups);
-            it.c0 = (int)(idx % groups) * kGroup;
-            it.c1 = min(nb, it.c0 + kGroup);
+            it.tile = (int)(idx / nch);
+            it.chunk = (int)(idx % nch);
             return it;
         }
         idx -= cnt;
@@ -169,8 +185,36 @@ __device__ __forceinline__ Item tc_item(const NetDev *nets, int nnets, int prec,
     return it;
 }
 
+// Epilogue of ncol (1 or 2) accumulators of one row: bias, clamp, store in
+// the compute type, row statistics.  dst0 = the row's 32 bytes of the first
+// output block in the output tile; the next block is 2048 elements further.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2)
+__device__ __forceinline__ void epilogue_cols(const float *v, int ncol, float bias, float ez, T *dst0,
+                                              bool valid, float &zmax, float &emax, float &ymax) {
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        if (q >= ncol) break;
+        __align__(16) T o[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const float z = v[q * 16 + i] + bias;
+            const float cz = clamp32(z);
+            o[i] = act_traits<T>::from_f(cz);
+            const float yf = act_traits<T>::to_f(o[i]);
+            zmax = fmaxf(zmax, z);
+            ymax = fmaxf(ymax, yf);
+            if (z > -ez && z < 32.0f + ez) emax = fmaxf(emax, __fadd_ru(ez, fabsf(yf - cz)));
+        }
+        if (valid) {
+            T *dst = dst0 + q * 2048;
+            *reinterpret_cast<uint4 *>(dst) = reinterpret_cast<const uint4 *>(o)[0];
+            *reinterpret_cast<uint4 *>(dst + 64) = reinterpret_cast<const uint4 *>(o)[1];
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 1)
     k_layer_tc(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches,
                int *abort_flag) {
     count_launch(launches);
@@ -182,13 +226,11 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
-            mbar_init(&sm.full[s], kLoaderWarps * 32);
+            mbar_init(&sm.full[s], 1);
             mbar_init(&sm.empty[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&sm.tfull[b], 1);
-            mbar_init(&sm.tempty[b], kEpiWarps * 32);
-        }
+        mbar_init(&sm.tfull, 1);
+        mbar_init(&sm.tempty, kEpiWarps * 32);
         mbar_init(&sm.fin, 1);
         sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -204,69 +246,71 @@ __global__ void __launch_bounds__(kThreads, 2)
     tc_fence_after();
     const uint32_t tmem = sm.tmem_base;
 
-    if (warp < kLoaderWarps) {
-        // ---------------- loaders: one row per thread -------------------
-        const int t = threadIdx.x;  // row within the tile, 0..127
-        const uint32_t a_off = (uint32_t)((t >> 3) * 256 + (t & 7) * 16);
-        uint32_t fill = 0;
-        bool ok = true;
-        for (int64_t idx = blockIdx.x; idx < total && ok; idx += gridDim.x) {
-            const Item it = tc_item(nets, nnets, prec, idx);
-            const NetDev &nd = nets[it.net];
-            const int l = nd.st->layer, R = nd.st->R, par = l & 1, N = nd.N;
-            const LayerDev &lw = nd.layers[l];
-            const T *in = (const T *)(l == 0 ? nd.y0 : nd.act[par]);
-            const int p = it.tile * kTileRows + t;
-            const char *row = p < R ? (const char *)(in + (int64_t)nd.pos[par][p] * N) : nullptr;
-            const char *bsrc = (const char *)lw.blk_b;
-            for (int c = it.c0; c < it.c1 && ok; ++c) {
-                const int b1 = lw.blk_ptr[c + 1];
-                for (int b = lw.blk_ptr[c]; b < b1; ++b) {
+    if (warp == kProducerWarp) {
+        // ---------------- producer: three bulk copies per stage ------------
+        if (lane == 0) {
+            uint32_t fill = 0;
+            bool ok = true;
+            for (int64_t idx = blockIdx.x; idx < total && ok; idx += gridDim.x) {
+                const Item it = tc_item(nets, nnets, prec, idx);
+                const NetDev &nd = nets[it.net];
+                const int l = nd.st->layer, N = nd.N;
+                const LayerDev &lw = nd.layers[l];
+                const char *in = (const char *)(l == 0 ? nd.y0 : nd.act[nd.st->in_buf]);
+                const char *tile = in + (int64_t)it.tile * (N / 16) * kTileBytes;
+                const int s0 = lw.tc_chunk_ptr[it.chunk], s1 = lw.tc_chunk_ptr[it.chunk + 1];
+                for (int q = s0; q < s1; ++q) {
+                    const int4 st = lw.tc_stage[q];  // a_first, a_count, b_first, n_mma
                     const uint32_t s = fill % kStages, u = fill / kStages;
                     if (u > 0 && !mbar_wait(&sm.empty[s], (u - 1) & 1, sm)) { ok = false; break; }
-                    const uint32_t st = smem_u32(sm.stage[s]);
-                    if (row) {
-                        const char *src = row + (int64_t)lw.blk_row[b] * 32;
-                        cp_async16(st + a_off, src);
-                        cp_async16(st + a_off + 128, src + 16);
-                    }
-                    if (t < 32) cp_async16(st + kStageA + t * 16, bsrc + (int64_t)b * kStageB + t * 16);
-                    cp_async_arrive_noinc(&sm.full[s]);
+                    const uint32_t base = smem_u32(sm.stage[s]);
+                    const uint32_t code_bytes = (uint32_t)((st.w + 7) & ~7) * 2;
+                    mbar_expect_tx(&sm.full[s], (uint32_t)st.y * kTileBytes + (uint32_t)st.w * kBBytes + code_bytes);
+                    bulk_load(base, tile + (int64_t)st.x * kTileBytes, (uint32_t)st.y * kTileBytes, &sm.full[s]);
+                    bulk_load(base + kStageA, (const char *)lw.tc_b + (int64_t)st.z * kBBytes, (uint32_t)st.w * kBBytes,
+                              &sm.full[s]);
+                    bulk_load(base + kStageA + kStageB, lw.tc_code + st.z, code_bytes, &sm.full[s]);
                     ++fill;
                 }
             }
+            // no bulk copy may still be writing shared memory when the CTA exits:
+            // wait (bounded) for the last fill of every stage
+            const uint32_t first = fill > (uint32_t)kStages ? fill - kStages : 0u;
+            for (uint32_t f = first; f < fill; ++f) {
+                const long long t0 = clock64();
+                while (!mbar_try_wait(&sm.full[f % kStages], (f / kStages) & 1) && clock64() - t0 < kWaitCycles) {
+                }
+            }
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
     } else if (warp == kMmaWarp) {
         // ---------------- MMA issuer ---------------------------------------
         if (lane == 0) {
-            const uint32_t idesc = instr_desc(sizeof(T) == 2 && prec == COSPDNN_PREC_BF16 ? 1u : 0u);
+            const uint32_t idesc = instr_desc(prec == COSPDNN_PREC_BF16 ? 1u : 0u);
             uint32_t fill = 0, iter = 0;
             bool ok = true;
             for (int64_t idx = blockIdx.x; idx < total && ok; idx += gridDim.x, ++iter) {
                 const Item it = tc_item(nets, nnets, prec, idx);
                 const NetDev &nd = nets[it.net];
                 const LayerDev &lw = nd.layers[nd.st->layer];
-                const uint32_t buf = iter & 1;
-                if (iter >= 2 && !mbar_wait(&sm.tempty[buf], ((iter >> 1) - 1) & 1, sm)) { ok = false; break; }
+                if (iter >= 1 && !mbar_wait(&sm.tempty, (iter - 1) & 1, sm)) { ok = false; break; }
                 tc_fence_after();
-                for (int c = it.c0; c < it.c1 && ok; ++c) {
-                    const uint32_t d = tmem + buf * (kGroup * 16) + (uint32_t)(c - it.c0) * 16;
-                    uint32_t acc = 0;
-                    const int b1 = lw.blk_ptr[c + 1];
-                    for (int b = lw.blk_ptr[c]; b < b1; ++b) {
-                        const uint32_t s = fill % kStages, u = fill / kStages;
-                        if (!mbar_wait(&sm.full[s], u & 1, sm)) { ok = false; break; }
-                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                        tc_fence_after();
-                        const uint32_t st = smem_u32(sm.stage[s]);
-                        mma_f16(d, smem_desc(st), smem_desc(st + kStageA), idesc, acc);
-                        mma_commit(&sm.empty[s]);
-                        acc = 1;
-                        ++fill;
+                const int s0 = lw.tc_chunk_ptr[it.chunk], s1 = lw.tc_chunk_ptr[it.chunk + 1];
+                for (int q = s0; q < s1; ++q) {
+                    const int n_mma = lw.tc_stage[q].w;
+                    const uint32_t s = fill % kStages, u = fill / kStages;
+                    if (!mbar_wait(&sm.full[s], u & 1, sm)) { ok = false; break; }
+                    const uint32_t base = smem_u32(sm.stage[s]);
+                    const uint16_t *code = reinterpret_cast<const uint16_t *>(sm.stage[s] + kStageA + kStageB);
+                    for (int j = 0; j < n_mma; ++j) {
+                        const uint32_t c = code[j];
+                        mma_f16(tmem + ((c >> 3) & 31u) * 16u, smem_desc(base + (c & 7u) * kTileBytes),
+                                smem_desc(base + kStageA + (uint32_t)j * kBBytes), idesc, (c >> 8) ? 0u : 1u);
                     }
+                    mma_commit(&sm.empty[s]);
+                    ++fill;
                 }
-                if (ok) mma_commit(&sm.tfull[buf]);
+                if (ok) mma_commit(&sm.tfull);
             }
             // every MMA this thread issued has completed before TMEM is freed
             mma_commit(&sm.fin);
@@ -279,14 +323,14 @@ __global__ void __launch_bounds__(kThreads, 2)
         // ---------------- epilogue: TMEM lane = row ---------------------------
         const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
         const int r = quarter * 32 + lane;
+        const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
         uint32_t iter = 0;
         for (int64_t idx = blockIdx.x; idx < total; idx += gridDim.x, ++iter) {
             const Item it = tc_item(nets, nnets, prec, idx);
             const NetDev &nd = nets[it.net];
             const int l = nd.st->layer, R = nd.st->R, par = l & 1, N = nd.N;
             const LayerDev &lw = nd.layers[l];
-            const uint32_t buf = iter & 1;
-            if (!mbar_wait(&sm.tfull[buf], (iter >> 1) & 1, sm)) break;
+            if (!mbar_wait(&sm.tfull, iter & 1, sm)) break;
             tc_fence_after();
             const int p = it.tile * kTileRows + r;
             const bool valid = p < R;
@@ -294,34 +338,23 @@ __global__ void __launch_bounds__(kThreads, 2)
                                                    fast_steps(nd, lw))
                                    : 0.0f;
             float zmax = -INFINITY, emax = 0.0f, ymax = 0.0f;
-            T *out = (T *)nd.act[par ^ 1] + (int64_t)(valid ? p : 0) * N;
-            for (int c = it.c0; c < it.c1; ++c) {
-                float v[16];
-                if (lw.blk_ptr[c + 1] > lw.blk_ptr[c]) {
-                    tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + buf * (kGroup * 16) + (uint32_t)(c - it.c0) * 16, v);
-                } else {
+            T *out = (T *)nd.act[nd.st->in_buf ^ 1];
+            const uint32_t used = lw.tc_used[it.chunk];
+            const int c0 = it.chunk * kChunk, ncol = min(kChunk, N / 16 - c0);
+            for (int j = 0; j < ncol; j += 2) {
+                float v[32];
+                tmem_ld32(tmem + lane_addr + (uint32_t)j * 16u, v);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) v[i] = 0.0f;
-                }
-                __align__(16) T o[16];
+                for (int q = 0; q < 2; ++q)
+                    if (!((used >> (j + q)) & 1u)) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float z = v[i] + nd.bias;
-                    const float cz = clamp32(z);
-                    o[i] = act_traits<T>::from_f(cz);
-                    const float yf = act_traits<T>::to_f(o[i]);
-                    zmax = fmaxf(zmax, z);
-                    ymax = fmaxf(ymax, yf);
-                    if (z > -ez && z < 32.0f + ez) emax = fmaxf(emax, __fadd_ru(ez, fabsf(yf - cz)));
-                }
-                if (valid) {
-                    uint4 *dst = reinterpret_cast<uint4 *>(out + c * 16);
-                    dst[0] = reinterpret_cast<const uint4 *>(o)[0];
-                    dst[1] = reinterpret_cast<const uint4 *>(o)[1];
-                }
+                        for (int i = 0; i < 16; ++i) v[q * 16 + i] = 0.0f;
+                    }
+                epilogue_cols<T>(v, min(2, ncol - j), nd.bias, ez, out + act_index(1, N, valid ? p : 0, (c0 + j) * 16),
+                                 valid, zmax, emax, ymax);
             }
             tc_fence_before();
-            mbar_arrive(&sm.tempty[buf]);
+            mbar_arrive(&sm.tempty);
             if (valid) {
                 atomicMax(&nd.stat[3 * p], f2ord(zmax));
                 atomicMax(&nd.stat[3 * p + 1], __float_as_uint(emax));
@@ -338,70 +371,110 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (threadIdx.x == 0 && sm.abort) atomicExch(abort_flag, 1);
 }
 
+template <typename D>
+int upload(const std::vector<D> &h, const D **dptr, std::vector<void *> &owned) {
+    void *p = nullptr;
+    CSP_CUDA(cudaMalloc(&p, std::max<size_t>(16, h.size() * sizeof(D))));
+    owned.push_back(p);
+    if (!h.empty()) CSP_CUDA(cudaMemcpy(p, h.data(), h.size() * sizeof(D), cudaMemcpyHostToDevice));
+    *dptr = (const D *)p;
+    return COSPDNN_OK;
+}
+
 }  // namespace
 
 bool tc_supported(int neuron) { return neuron > 0 && neuron % 16 == 0; }
 
+// Builds the chunked, input-stationary MMA schedule of one layer (see LayerDev).
 int tc_build_blocks(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx,
                     const std::vector<float> &vals, int N, int prec, LayerDev &ld, std::vector<void *> &owned) {
-    const int nb = N / 16;
-    std::vector<int32_t> ptr(nb + 1, 0), brow;
+    const int nb = N / 16, nchunks = (nb + kChunk - 1) / kChunk;
+    std::vector<int32_t> chunk_ptr(nchunks + 1, 0);
+    std::vector<int4> stages;
+    std::vector<uint16_t> codes;
     std::vector<uint16_t> bvals;
+    std::vector<uint32_t> used(nchunks, 0u);
     int maxb = 0;
-    std::vector<int> slot(nb, -1);
-    for (int c = 0; c < nb; ++c) {
-        std::vector<int> used;
-        for (int n = 0; n < 16; ++n) {
-            const int j = c * 16 + n;
-            for (int p = colptr[j]; p < colptr[j + 1]; ++p) {
-                const int ib = rowidx[p] / 16;
-                if (slot[ib] < 0) { slot[ib] = 0; used.push_back(ib); }
-            }
+    auto to_bits = [prec](float v) {
+        uint16_t bits;
+        if (prec == COSPDNN_PREC_BF16) {
+            __nv_bfloat16 h = __float2bfloat16_rn(v);
+            std::memcpy(&bits, &h, 2);
+        } else {
+            __half h = __float2half_rn(v);
+            std::memcpy(&bits, &h, 2);
         }
-        std::sort(used.begin(), used.end());
-        const size_t base = brow.size();
-        for (size_t q = 0; q < used.size(); ++q) slot[used[q]] = (int)(base + q);
-        brow.insert(brow.end(), used.begin(), used.end());
-        bvals.resize(brow.size() * 256, 0);
-        for (int n = 0; n < 16; ++n) {
-            const int j = c * 16 + n;
-            for (int p = colptr[j]; p < colptr[j + 1]; ++p) {
-                const int i = rowidx[p], k = i % 16;
-                const size_t blk = (size_t)slot[i / 16];
-                // element (n, k) of the K-major B operand: 8x16-byte core matrices,
-                // K halves 128 bytes apart, 8-row groups 256 bytes apart
-                const size_t off = (size_t)(n / 8) * 128 + (size_t)(k / 8) * 64 + (size_t)(n % 8) * 8 + (size_t)(k % 8);
-                uint16_t bits;
-                if (prec == COSPDNN_PREC_BF16) {
-                    __nv_bfloat16 h = __float2bfloat16_rn(vals[p]);
-                    std::memcpy(&bits, &h, 2);
-                } else {
-                    __half h = __float2half_rn(vals[p]);
-                    std::memcpy(&bits, &h, 2);
+        return bits;
+    };
+    for (int h = 0; h < nchunks; ++h) {
+        // (input block, column in chunk) -> dense 16x16 block, ordered by input block
+        std::map<std::pair<int, int>, std::vector<uint16_t>> blocks;
+        for (int jc = 0; jc < kChunk && h * kChunk + jc < nb; ++jc) {
+            const int c = h * kChunk + jc;
+            int nblk = 0;
+            for (int n = 0; n < 16; ++n) {
+                const int j = c * 16 + n;
+                for (int p = colptr[j]; p < colptr[j + 1]; ++p) {
+                    const int i = rowidx[p], k = i % 16;
+                    auto key = std::make_pair(i / 16, jc);
+                    auto itb = blocks.find(key);
+                    if (itb == blocks.end()) {
+                        itb = blocks.emplace(key, std::vector<uint16_t>(256, 0)).first;
+                        ++nblk;
+                    }
+                    // element (n, k) of the K-major B operand: 8x16-byte core matrices,
+                    // K halves 128 bytes apart, 8-row groups 256 bytes apart
+                    const size_t off = (size_t)(n / 8) * 128 + (size_t)(k / 8) * 64 + (size_t)(n % 8) * 8 + (size_t)(k % 8);
+                    itb->second[off] = to_bits(vals[p]);
                 }
-                bvals[blk * 256 + off] = bits;
             }
+            maxb = std::max(maxb, nblk);
+            if (nblk) used[h] |= 1u << jc;
         }
-        for (int ib : used) slot[ib] = -1;
-        ptr[c + 1] = (int32_t)brow.size();
-        maxb = std::max(maxb, (int)used.size());
+        // stages: runs of input blocks (<= kMaxA wide, gaps <= kMaxGap), <= kMaxMma MMAs
+        uint32_t seen = 0u;
+        auto it = blocks.begin();
+        while (it != blocks.end()) {
+            const int a_first = it->first.first;
+            int a_last = a_first;
+            std::vector<decltype(it)> members;
+            while (it != blocks.end()) {
+                const int i = it->first.first;
+                auto jt = it;
+                int cnt = 0;
+                while (jt != blocks.end() && jt->first.first == i) { ++jt; ++cnt; }
+                const bool fits = (i - a_first + 1 <= kMaxA) && (i - a_last <= kMaxGap + 1) &&
+                                  ((int)members.size() + cnt <= kMaxMma);
+                if (!members.empty() && !fits) break;
+                for (auto kt = it; kt != jt; ++kt) members.push_back(kt);
+                a_last = i;
+                it = jt;
+            }
+            const int b_first = (int)((codes.size() + 7) / 8 * 8);  // code copies start 16-byte aligned
+            codes.resize(b_first, 0);
+            bvals.resize((size_t)b_first * 256, 0);
+            for (auto &m : members) {
+                const int i = m->first.first, jc = m->first.second;
+                const bool first = !((seen >> jc) & 1u);
+                seen |= 1u << jc;
+                codes.push_back((uint16_t)((i - a_first) | (jc << 3) | (first ? 256 : 0)));
+                bvals.insert(bvals.end(), m->second.begin(), m->second.end());
+            }
+            stages.push_back(make_int4(a_first, a_last - a_first + 1, b_first, (int)members.size()));
+        }
+        chunk_ptr[h + 1] = (int32_t)stages.size();
     }
-    int32_t *dptr = nullptr, *drow = nullptr;
-    void *dvals = nullptr;
-    CSP_CUDA(cudaMalloc(&dptr, sizeof(int32_t) * ptr.size()));
-    owned.push_back(dptr);
-    CSP_CUDA(cudaMalloc(&drow, sizeof(int32_t) * std::max<size_t>(1, brow.size())));
-    owned.push_back(drow);
-    CSP_CUDA(cudaMalloc(&dvals, 2 * std::max<size_t>(256, bvals.size())));
-    owned.push_back(dvals);
-    CSP_CUDA(cudaMemcpy(dptr, ptr.data(), sizeof(int32_t) * ptr.size(), cudaMemcpyHostToDevice));
-    if (!brow.empty()) {
-        CSP_CUDA(cudaMemcpy(drow, brow.data(), sizeof(int32_t) * brow.size(), cudaMemcpyHostToDevice));
-        CSP_CUDA(cudaMemcpy(dvals, bvals.data(), 2 * bvals.size(), cudaMemcpyHostToDevice));
-    }
-    ld.blk_ptr = dptr;
-    ld.blk_row = drow;
-    ld.blk_b = dvals;
+    codes.resize((codes.size() + 7) / 8 * 8 + 8, 0);  // room for the last aligned code copy
+    bvals.resize(std::max<size_t>(bvals.size(), codes.size() * 256), 0);
+    int rc;
+    if ((rc = upload(chunk_ptr, &ld.tc_chunk_ptr, owned))) return rc;
+    if ((rc = upload(stages, &ld.tc_stage, owned))) return rc;
+    if ((rc = upload(codes, &ld.tc_code, owned))) return rc;
+    if ((rc = upload(used, &ld.tc_used, owned))) return rc;
+    const uint16_t *bptr = nullptr;
+    if ((rc = upload(bvals, &bptr, owned))) return rc;
+    ld.tc_b = bptr;
+    ld.tc_nchunks = nchunks;
     ld.max_blocks = maxb;
     return COSPDNN_OK;
 }
@@ -410,10 +483,7 @@ int tc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long lon
                   int sms) {
     k.fn = prec == COSPDNN_PREC_BF16 ? (void *)k_layer_tc<__nv_bfloat16> : (void *)k_layer_tc<__half>;
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
-    int per_sm = 0;
-    CSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, kThreads, kSmemBytes));
-    per_sm = std::max(1, std::min(per_sm, 512 / kTmemCols));
-    k.grid = dim3(sms * per_sm);
+    k.grid = dim3(sms);  // one CTA (all of TMEM) per SM
     k.block = dim3(kThreads);
     k.smem = kSmemBytes;
     k.arg(nets).arg(nnets).arg(prec).arg(launches).arg(abort_flag);
