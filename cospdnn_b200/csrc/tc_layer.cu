@@ -301,11 +301,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t s = fill % kStages, u = fill / kStages;
                     if (!mbar_wait(&sm.full[s], u & 1, sm)) { ok = false; break; }
                     const uint32_t base = smem_u32(sm.stage[s]);
-                    const uint16_t *code = reinterpret_cast<const uint16_t *>(sm.stage[s] + kStageA + kStageB);
-                    for (int j = 0; j < n_mma; ++j) {
-                        const uint32_t c = code[j];
-                        mma_f16(tmem + ((c >> 3) & 31u) * 16u, smem_desc(base + (c & 7u) * kTileBytes),
-                                smem_desc(base + kStageA + (uint32_t)j * kBBytes), idesc, (c >> 8) ? 0u : 1u);
+                    const uint64_t adesc0 = smem_desc(base), bdesc0 = smem_desc(base + kStageA);
+                    const uint4 *code8 = reinterpret_cast<const uint4 *>(sm.stage[s] + kStageA + kStageB);
+                    // 8 MMAs per step, each with its own operand registers, so an MMA
+                    // still reading its descriptors never holds up the next one
+                    for (int j0 = 0; j0 < n_mma; j0 += 8) {
+                        const uint4 cv = code8[j0 >> 3];
+                        const uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            if (j0 + q < n_mma) {
+                                const uint32_t c = (cw[q >> 1] >> ((q & 1) * 16)) & 0xFFFFu;
+                                mma_f16(tmem + ((c >> 3) & 31u) * 16u, adesc0 + (uint64_t)((c & 7u) * (kTileBytes >> 4)),
+                                        bdesc0 + (uint64_t)((j0 + q) * (kBBytes >> 4)), idesc, (c >> 8) ? 0u : 1u);
+                            }
+                        }
                     }
                     mma_commit(&sm.empty[s]);
                     ++fill;
@@ -449,6 +459,17 @@ int tc_build_blocks(const std::vector<int32_t> &colptr, const std::vector<int32_
                 for (auto kt = it; kt != jt; ++kt) members.push_back(kt);
                 a_last = i;
                 it = jt;
+            }
+            // round-robin over accumulators: the k-th MMA of every column before
+            // any (k+1)-th, so MMAs into the same accumulator are far apart
+            {
+                std::map<int, int> occ;
+                std::vector<std::pair<int, int>> key(members.size());
+                for (size_t q = 0; q < members.size(); ++q) key[q] = {occ[members[q]->first.second]++, (int)q};
+                std::stable_sort(key.begin(), key.end());
+                std::vector<decltype(it)> ordered;
+                for (auto &kq : key) ordered.push_back(members[kq.second]);
+                members.swap(ordered);
             }
             const int b_first = (int)((codes.size() + 7) / 8 * 8);  // code copies start 16-byte aligned
             codes.resize(b_first, 0);
