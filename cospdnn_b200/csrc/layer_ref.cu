@@ -4,7 +4,7 @@
 //                             (src/kernels/kernel.cu:129-172, src/cospdnn.cu:236-276)
 // These keep the reference's [feature][batch] activations so a harness can
 // call them where the reference kernels are launched.  The whole-network
-// engine (engine.cu) uses its own row-major layout instead.
+// engine (engine.cu) keeps its own layouts (row-major or MMA tiles).
 #include <algorithm>
 #include <mutex>
 
@@ -243,4 +243,50 @@ extern "C" int cospdnn_prune_compact(const float *C, int neuron, int batch, floa
     CSP_CHECK(!(flags & ~1u), COSPDNN_ERR_INVALID, "cospdnn_prune_compact: unknown flag");
     return prune_compact_impl(C, neuron, batch, threshold, A_out, category, map_in, map_out,
                               count_dev, flags, (int *)workspace, (cudaStream_t)stream);
+}
+
+// ---- allocation-free pruning entry ----------------------------------------
+// Same computation as cospdnn_prune_compact, with the per-column flag
+// scratch in a file-scope device array instead of caller-provided memory.
+namespace cospdnn {
+namespace {
+constexpr int kNoAllocMaxBatch = 1 << 20;  // columns; 4 MiB of scratch on every GPU that loads the library
+__device__ __align__(256) int g_prune_scratch[kNoAllocMaxBatch];
+std::mutex g_scratch_mu;
+int *g_scratch_addr[1024];  // device address of g_prune_scratch, per device ordinal
+
+// Host code cannot use g_prune_scratch's name as a device address: ask the
+// runtime for it once per device, with that device current.
+int scratch_for_current_device(int **out) {
+    int dev = 0;
+    CSP_CUDA(cudaGetDevice(&dev));
+    CSP_CHECK(dev >= 0 && dev < 1024, COSPDNN_ERR_UNSUPPORTED, "prune_compact_noalloc: device ordinal too large");
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_prune_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "prune_compact_noalloc: cudaGetSymbolAddress");
+        g_scratch_addr[dev] = (int *)p;
+    }
+    *out = g_scratch_addr[dev];
+    return COSPDNN_OK;
+}
+}  // namespace
+}  // namespace cospdnn
+
+extern "C" int cospdnn_prune_compact_noalloc(const float *C, int neuron, int batch, float threshold,
+                                             void *A_out, int *category, const int *map_in, int *map_out,
+                                             int *count_dev, unsigned flags, void *stream) {
+    CSP_CHECK(C && A_out && category && map_out && count_dev, COSPDNN_ERR_INVALID,
+              "cospdnn_prune_compact_noalloc: null pointer");
+    CSP_CHECK(neuron > 0 && batch > 0, COSPDNN_ERR_INVALID, "cospdnn_prune_compact_noalloc: bad sizes");
+    CSP_CHECK(batch <= kNoAllocMaxBatch, COSPDNN_ERR_INVALID,
+              "cospdnn_prune_compact_noalloc: batch exceeds the 1048576-column scratch");
+    CSP_CHECK(!(flags & ~1u), COSPDNN_ERR_INVALID, "cospdnn_prune_compact_noalloc: unknown flag");
+    int *ws = nullptr;
+    const int rc = scratch_for_current_device(&ws);
+    if (rc) return rc;
+    // prune_compact_impl clears the flags it uses (an async memset, no allocation)
+    return prune_compact_impl(C, neuron, batch, threshold, A_out, category, map_in, map_out, count_dev, flags, ws,
+                              (cudaStream_t)stream);
 }

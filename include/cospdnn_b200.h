@@ -77,7 +77,8 @@ int cospdnn_layer(const void *A, const void *B, float *C, const int *fuse, const
  *   A_out [neuron][stride], stride = count rounded up to a multiple of 128,
  *   gets the surviving columns and zero padding; with COSPDNN_PRUNE_OUT_HALF_HILO
  *   A_out is half [2*neuron][stride] hi/lo rows, ready for cospdnn_layer.
- * A_out, category and map_out need room for batch columns.  `workspace` is
+ * A_out needs room for batch columns rounded up to a multiple of 128,
+ * category and map_out for batch entries.  `workspace` is
  * device memory of cospdnn_prune_workspace_bytes(batch) bytes, owned by the
  * caller.  Asynchronous; read *count_dev after synchronizing.
  */
@@ -86,6 +87,24 @@ size_t cospdnn_prune_workspace_bytes(int batch);
 int cospdnn_prune_compact(const float *C, int neuron, int batch, float threshold, void *A_out,
                           int *category, const int *map_in, int *map_out, int *count_dev,
                           unsigned flags, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Allocation-free variant of cospdnn_prune_compact (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: code that must not
+ * implicitly synchronize the device (cudaMalloc/cudaFree can), code whose
+ * device memory is owned by another allocator or fixed budget, or code that
+ * simply has no place to keep a workspace between calls.  Same arguments and
+ * results as cospdnn_prune_compact minus the workspace: the per-column flags
+ * live in a file-scope device array of 1048576 ints (4 MiB), held on every
+ * GPU that loads this library until the process exits; batch > 1048576 is
+ * rejected with COSPDNN_ERR_INVALID.  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress, with the device
+ * current), so make the first call on each device before any stream capture.
+ * Every call clears the flags it uses; all calls share the one array, so
+ * calls that overlap on the GPU (other streams, other threads) race.  No
+ * cudaMalloc, cudaFree or other allocating call is made. */
+int cospdnn_prune_compact_noalloc(const float *C, int neuron, int batch, float threshold,
+                                  void *A_out, int *category, const int *map_in, int *map_out,
+                                  int *count_dev, unsigned flags, void *stream);
 
 /* ------------------------------------------------------------------------
  * Whole-network engine.  Replaces the host layer loop test_graph_challenge_tc
