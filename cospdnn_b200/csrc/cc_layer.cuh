@@ -1,0 +1,26 @@
+// CUDA-core row-tile layer kernel interface (implementation in cc_layer.cu).
+#pragma once
+
+#include <vector>
+
+#include "engine.cuh"
+
+namespace cospdnn {
+
+// Row-tile height TR (activation layout TR) for a CUDA-core net of width N in
+// precision `prec`, or 0 when a tile of 16-byte feature columns does not fit
+// in shared memory (the net then uses the row-major gather kernel).
+int cc_tile_rows(int N, int prec);
+// Builds the entry list of one layer from its CSC (conflict-free order for
+// tile height TR) and uploads it.
+int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx,
+                     const std::vector<float> &vals, int N, int prec, int TR, LayerDev &ld,
+                     std::vector<void *> &owned);
+// Launch description of the tile kernel for the CUDA-core row-tile nets of
+// precision `prec`; max_tile_bytes = largest N*TR*element size among them.
+int cc_layer_spec(KSpec &spec, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms,
+                  size_t max_tile_bytes);
+// Bytes of one row tile.
+inline size_t cc_tile_bytes(int N, int prec, int TR) { return (size_t)N * TR * (prec == COSPDNN_PREC_FP32 ? 4 : 2); }
+
+}  // namespace cospdnn

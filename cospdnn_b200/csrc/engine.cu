@@ -7,6 +7,7 @@
 #include <memory>
 #include <vector>
 
+#include "cc_layer.cuh"
 #include "engine_kernels.cuh"
 #include "tc_layer.cuh"
 
@@ -16,7 +17,7 @@ namespace {
 
 // ---- input conversion: any format -> compute type, per-row error and max --
 template <typename T, int FMT>
-__global__ void k_convert_input(const void *__restrict__ src, int rows, int N, int tiled, T *__restrict__ y0,
+__global__ void k_convert_input(const void *__restrict__ src, int rows, int N, int layout, T *__restrict__ y0,
                                 float *__restrict__ y0_f32, float *__restrict__ err0,
                                 float *__restrict__ mx0) {
     // one warp per row
@@ -31,7 +32,7 @@ __global__ void k_convert_input(const void *__restrict__ src, int rows, int N, i
             else if (FMT == COSPDNN_INPUT_F32) x = ((const float *)src)[r * N + j];
             else x = (float)((((const uint8_t *)src)[r * (N / 8) + (j >> 3)] >> (j & 7)) & 1u);
             const T v = act_traits<T>::from_f(x);
-            y0[act_index(tiled, N, r, j)] = v;
+            y0[act_index(layout, N, r, j)] = v;
             if (y0_f32) y0_f32[r * N + j] = x;
             e = fmaxf(e, fabsf(act_traits<T>::to_f(v) - x));
             m = fmaxf(m, fabsf(x));
@@ -54,7 +55,7 @@ __global__ void k_gather_final(const NetDev *__restrict__ nd_p, float *__restric
     const int64_t total = (int64_t)min((int64_t)R, max_rows) * N;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t q = i / N, j = i % N;
-        out[i] = act_traits<T>::to_f(act[act_index(nd.tiled, N, q, (int)j)]);
+        out[i] = act_traits<T>::to_f(act[act_index(nd.layout, N, q, (int)j)]);
     }
 }
 
@@ -188,11 +189,20 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
     if (net.dev.kernel == COSPDNN_KERNEL_TCGEN05) {
         int rc = tc_build_blocks(h.colptr, h.rowidx, h.vals, N, net.d.precision, ld, e->owned);
         if (rc) return rc;
+    } else if (const int TR = cc_tile_rows(N, net.d.precision)) {
+        int rc = cc_build_entries(h.colptr, h.rowidx, h.vals, N, net.d.precision, TR, ld, e->owned);
+        if (rc) return rc;
     }
     return COSPDNN_OK;
 }
 
-int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std::vector<int> &tc_precs) {
+// Precisions of the nets on each layer kernel.
+struct KernelSets {
+    std::vector<int> plain, cc, tc;
+    size_t cc_tile_bytes = 0;  // largest row tile of the cc nets
+};
+
+int make_specs(cospdnn_engine *e, const KernelSets &ks) {
     int sms = 148;
     CSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
     const int nn = (int)e->nets.size();
@@ -204,7 +214,7 @@ int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std
     k0.grid = dim3(sms * 4);
     k0.block = dim3(256);
     k0.arg(nets).arg(nn).arg(launches).arg(guard).arg(e->abort_flag);
-    for (int prec : plain_precs) {
+    for (int prec : ks.plain) {
         KSpec k;
         k.fn = prec == COSPDNN_PREC_FP32 ? (void *)k_layer_plain<float>
              : prec == COSPDNN_PREC_FP16 ? (void *)k_layer_plain<__half>
@@ -216,7 +226,13 @@ int make_specs(cospdnn_engine *e, const std::vector<int> &plain_precs, const std
         k.arg(nets).arg(nn).arg(prec).arg(launches);
         e->layer_specs.push_back(std::move(k));
     }
-    for (int prec : tc_precs) {
+    for (int prec : ks.cc) {
+        KSpec k;
+        int rc = cc_layer_spec(k, nets, nn, prec, launches, sms, ks.cc_tile_bytes);
+        if (rc) return rc;
+        e->layer_specs.push_back(std::move(k));
+    }
+    for (int prec : ks.tc) {
         KSpec k;
         int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, sms);
         if (rc) return rc;
@@ -266,10 +282,10 @@ int launch(KSpec &k, cudaStream_t s) {
     return COSPDNN_OK;
 }
 
-int build_graph(cospdnn_engine *e, const std::vector<int> &plain_precs, const std::vector<int> &tc_precs) {
+int build_graph(cospdnn_engine *e, const KernelSets &ks) {
     CSP_CUDA(cudaGraphCreate(&e->graph, 0));
     CSP_CUDA(cudaGraphConditionalHandleCreate(&e->loop, e->graph, 1, cudaGraphCondAssignDefault));
-    int rc = make_specs(e, plain_precs, tc_precs);
+    int rc = make_specs(e, ks);
     if (rc) return rc;
     cudaGraphNode_t k0;
     if ((rc = add_node(e->graph, &k0, nullptr, 0, e->k0))) return rc;
@@ -332,8 +348,10 @@ extern "C" int cospdnn_engine_add_net(cospdnn_engine *e, const cospdnn_net_desc 
     net.layers.resize(d->layers);
     int k = d->kernel;
     if (k == COSPDNN_KERNEL_AUTO)
-        k = (d->precision != COSPDNN_PREC_FP32 && tc_supported(d->neuron)) ? COSPDNN_KERNEL_TCGEN05
-                                                                         : COSPDNN_KERNEL_CUDA_CORE;
+        k = (cc_tile_rows(d->neuron, d->precision) == 0 && d->precision != COSPDNN_PREC_FP32 &&
+             tc_supported(d->neuron))
+                ? COSPDNN_KERNEL_TCGEN05
+                : COSPDNN_KERNEL_CUDA_CORE;
     if (k == COSPDNN_KERNEL_TCGEN05)
         CSP_CHECK(tc_supported(d->neuron), COSPDNN_ERR_UNSUPPORTED, "add_net: tcgen05 kernel needs neuron % 16 == 0");
     net.dev.kernel = k;
@@ -423,14 +441,19 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     CSP_CHECK(!e->built, COSPDNN_ERR_STATE, "build: already built");
     CSP_CHECK(!e->nets.empty(), COSPDNN_ERR_STATE, "build: no networks");
     DeviceGuard g(e->device);
-    std::vector<int> plain, tc;
+    KernelSets ks;
     for (Net &n : e->nets) {
         for (int l = 0; l < n.d.layers; ++l)
             CSP_CHECK(n.layers[l].set, COSPDNN_ERR_STATE, "build: a layer's weights were not set");
         e->max_n = std::max(e->max_n, n.d.neuron);
         e->max_layers = std::max(e->max_layers, n.d.layers);
-        auto &v = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? tc : plain;
+        // activation layout: MMA tiles (tcgen05), row tiles (CUDA-core tile
+        // kernel) or row-major (CUDA-core gather kernel, rows too wide for a tile)
+        n.dev.layout = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? 1 : cc_tile_rows(n.d.neuron, n.d.precision);
+        auto &v = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? ks.tc : n.dev.layout >= 2 ? ks.cc : ks.plain;
         if (std::find(v.begin(), v.end(), n.d.precision) == v.end()) v.push_back(n.d.precision);
+        if (n.dev.layout >= 2)
+            ks.cc_tile_bytes = std::max(ks.cc_tile_bytes, cc_tile_bytes(n.d.neuron, n.d.precision, n.dev.layout));
     }
     for (Net &n : e->nets) {
         const int N = n.d.neuron, R = std::max(1, n.d.rows);
@@ -452,7 +475,6 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         d.bias = n.d.bias;
         d.tau = n.d.threshold;
         d.layers = n.d_layers;
-        d.tiled = d.kernel == COSPDNN_KERNEL_TCGEN05;
         const size_t rows_pad = (size_t)(R + 127) / 128 * 128;
         const size_t es = elem_size(d.prec), act = rows_pad * N * es;
         d.y0 = dalloc<char>(act, e->owned);
@@ -506,7 +528,7 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     CSP_CUDA(cudaMemset(e->abort_flag, 0, sizeof(int)));
     CSP_CUDA(cudaMemset(e->finished, 0, sizeof(unsigned int)));
     CSP_CUDA(cudaMemset(e->launches, 0, sizeof(unsigned long long)));
-    int rc = build_graph(e, plain, tc);
+    int rc = build_graph(e, ks);
     if (rc) return rc;
     CSP_CUDA(cudaDeviceSynchronize());
     e->built = true;
@@ -558,9 +580,9 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
 #define CSP_CONV(T)                                                                                      \
     do {                                                                                                 \
         T *dst = (T *)n.dev.y0;                                                                          \
-        if (format == COSPDNN_INPUT_U8) k_convert_input<T, COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, R, N, n.dev.tiled, dst, f32, err0, mx0); \
-        else if (format == COSPDNN_INPUT_F32) k_convert_input<T, COSPDNN_INPUT_F32><<<blocks, 256, 0, s>>>(src, R, N, n.dev.tiled, dst, f32, err0, mx0); \
-        else k_convert_input<T, COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, R, N, n.dev.tiled, dst, f32, err0, mx0); \
+        if (format == COSPDNN_INPUT_U8) k_convert_input<T, COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, R, N, n.dev.layout, dst, f32, err0, mx0); \
+        else if (format == COSPDNN_INPUT_F32) k_convert_input<T, COSPDNN_INPUT_F32><<<blocks, 256, 0, s>>>(src, R, N, n.dev.layout, dst, f32, err0, mx0); \
+        else k_convert_input<T, COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, R, N, n.dev.layout, dst, f32, err0, mx0); \
     } while (0)
     if (n.d.precision == COSPDNN_PREC_FP32) CSP_CONV(float);
     else if (n.d.precision == COSPDNN_PREC_FP16) CSP_CONV(__half);

@@ -58,6 +58,13 @@ struct LayerDev {
     const uint32_t *tc_used;
     int tc_nchunks;
     int max_blocks;  // max 16x16 blocks in one output block column (error bound)
+    // CUDA-core tile kernel (k_layer_cc): per output j, cc_k entries (input
+    // index, weight in the compute type) in a build-time order, zero-weight
+    // padding included; 16-byte groups of entries stored group-major,
+    // [group][j] (16-bit nets: 4 entries of idx | w << 16; FP32 nets:
+    // 2 entries of {idx, w bits}), so consecutive outputs are adjacent.
+    const uint4 *cc_w;
+    int cc_k;
     float S;         // max_j sum_i |W_ij|
     float dW;        // max_j sum_i |W'_ij - W_ij|, W' = weights in the compute type
 };
@@ -82,7 +89,7 @@ struct NetDev {
     const float *y0_f32;     // exact input when the compute type cannot hold it (else NULL)
     const float *err0;       // [rows] bound on |y0(compute) - y0(exact)|
     const float *mx0;        // [rows] max |y0|
-    int tiled;               // activation layout: 0 row-major, 1 MMA tiles (see act_index)
+    int layout;              // activation layout: 0 row-major, 1 MMA tiles, >= 2 row tiles (see act_index)
     void *act[2];            // ping-pong activations, rows padded to a multiple of 128
     int32_t *cmap;           // [rows] compaction map: new row q <- output row cmap[q]
     int32_t *orig[2];        // list: original row id
@@ -99,17 +106,25 @@ struct NetDev {
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
 
 // Element index of (row, feature) in an activation buffer of width N.
-// Row-major: row*N + f.  MMA tiles (tcgen05 nets): rows in tiles of 128 and
-// features in blocks of 16; each (tile, block) is a contiguous 4 KB operand in
-// the canonical K-major core-matrix order of tcgen05 (8 rows x 16 bytes per
-// core matrix, the two 8-feature halves 128 bytes apart, 8-row groups 256
-// bytes apart), so one bulk copy brings a whole MMA A operand into shared
-// memory and the epilogue writes one output block as one such operand.
-__host__ __device__ __forceinline__ int64_t act_index(int tiled, int N, int64_t row, int f) {
-    if (!tiled) return row * N + f;
-    const int64_t tile = row >> 7;
-    const int m = (int)(row & 127), fb = f >> 4, k = f & 15;
-    return (tile * (N >> 4) + fb) * 2048 + (m >> 3) * 128 + (k >> 3) * 64 + (m & 7) * 8 + (k & 7);
+// layout 0, row-major: row*N + f.
+// layout 1, MMA tiles (tcgen05 nets): rows in tiles of 128 and features in
+// blocks of 16; each (tile, block) is a contiguous 4 KB operand in the
+// canonical K-major core-matrix order of tcgen05 (8 rows x 16 bytes per core
+// matrix, the two 8-feature halves 128 bytes apart, 8-row groups 256 bytes
+// apart), so one bulk copy brings a whole MMA A operand into shared memory
+// and the epilogue writes one output block as one such operand.
+// layout TR >= 2 (a power of two), row tiles (CUDA-core tile kernel): rows in
+// tiles of TR, feature-major inside a tile: (tile*N + f)*TR + row%TR, so a
+// tile is one contiguous block and the TR values of one feature are adjacent.
+__host__ __device__ __forceinline__ int64_t act_index(int layout, int N, int64_t row, int f) {
+    if (layout == 0) return row * N + f;
+    if (layout == 1) {
+        const int64_t tile = row >> 7;
+        const int m = (int)(row & 127), fb = f >> 4, k = f & 15;
+        return (tile * (N >> 4) + fb) * 2048 + (m >> 3) * 128 + (k >> 3) * 64 + (m & 7) * 8 + (k & 7);
+    }
+    const int64_t tile = row / layout;
+    return (tile * N + f) * layout + (row - tile * layout);
 }
 
 // Counts kernel launches of a run (one atomic per launch, block 0 thread 0).
@@ -138,7 +153,8 @@ __device__ __forceinline__ float z_error_bound(float e_in, float m_in, float S, 
 
 // Roundings per output of each fast kernel (see z_error_bound).
 __device__ __forceinline__ double fast_steps(const NetDev &n, const LayerDev &lw) {
-    // CUDA-core: one FMA rounding per term and one for the bias.  tcgen05:
+    // CUDA-core kernels: one FMA rounding per term (zero-weight padding is
+    // exact) and one for the bias.  tcgen05:
     // accumulation order inside the MMA is not specified, so allow two
     // roundings for every product of every block plus the bias.
     return n.kernel == COSPDNN_KERNEL_TCGEN05 ? 2.0 * (16.0 * lw.max_blocks + 2.0) : (double)(lw.K + 2);

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kPlainThreads)
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (nd.kernel != COSPDNN_KERNEL_CUDA_CORE || nd.prec != prec || nd.st->done) continue;
+        if (nd.kernel != COSPDNN_KERNEL_CUDA_CORE || nd.layout != 0 || nd.prec != prec || nd.st->done) continue;
         total += (nd.st->R + kPlainRows - 1) / kPlainRows;
     }
     for (int64_t unit = gwarp; unit < total; unit += nwarps) {
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kPlainThreads)
         int n = 0;
         for (; n < nnets; ++n) {
             const NetDev &nd = nets[n];
-            if (nd.kernel != COSPDNN_KERNEL_CUDA_CORE || nd.prec != prec || nd.st->done) continue;
+            if (nd.kernel != COSPDNN_KERNEL_CUDA_CORE || nd.layout != 0 || nd.prec != prec || nd.st->done) continue;
             const int64_t cnt = (nd.st->R + kPlainRows - 1) / kPlainRows;
             if (u < cnt) break;
             u -= cnt;
@@ -204,7 +204,7 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
     double *y = buf0, *z = buf1;
     for (int j = threadIdx.x; j < N; j += blockDim.x)
         y[j] = nd.y0_f32 ? (double)nd.y0_f32[(int64_t)orow * N + j]
-                         : act_traits<T>::to_d(((const T *)nd.y0)[act_index(nd.tiled, N, orow, j)]);
+                         : act_traits<T>::to_d(((const T *)nd.y0)[act_index(nd.layout, N, orow, j)]);
     __syncthreads();
     const double b = (double)nd.bias;
     for (int ll = 0; ll <= l; ++ll) {
@@ -229,7 +229,7 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
         T *out = (T *)nd.act[ib ^ 1];
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
             const T v = act_traits<T>::from_d(y[j]);
-            out[act_index(nd.tiled, N, p, j)] = v;
+            out[act_index(nd.layout, N, p, j)] = v;
             const double vd = act_traits<T>::to_d(v);
             emax = fmaxf(emax, __double2float_ru(fabs(vd - y[j])));
             ymax = fmaxf(ymax, (float)vd);
@@ -372,15 +372,43 @@ __global__ void __launch_bounds__(kCompactThreads)
 }
 
 // ---- K5: move the kept rows to the front of the next input buffer ---------
-// Row q of act[in_buf] <- row cmap[q] of act[in_buf ^ 1], in 16-byte pieces
-// (row-major: consecutive; MMA tiles: the two 8-feature halves of each block).
+// Row q of act[in_buf] <- row cmap[q] of act[in_buf ^ 1].
+// Row-major and MMA-tile nets: 16-byte pieces (row-major: consecutive; MMA
+// tiles: the two 8-feature halves of each block).  Row-tile nets: one CTA per
+// destination tile, which is written contiguously (feature-major, TR values
+// per feature; rows past the kept count are zero).
+template <typename E>
+__device__ __forceinline__ void copy_tile(const NetDev &nd, int tq, int64_t *s_src) {
+    const int N = nd.N, TR = nd.layout, ib = nd.st->in_buf, R = nd.st->copy_R;
+    const E *src = (const E *)nd.act[ib ^ 1];
+    E *dst = (E *)nd.act[ib] + (int64_t)tq * N * TR;
+    __syncthreads();
+    for (int r = threadIdx.x; r < TR; r += blockDim.x) {
+        const int q = tq * TR + r;
+        s_src[r] = q < R ? act_index(TR, N, nd.cmap[q], 0) : -1;
+    }
+    __syncthreads();
+    const int lg = __ffs(TR) - 1;
+    const int total = N * TR;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        const int r = i & (TR - 1), f = i >> lg;
+        const int64_t o = s_src[r];
+        dst[i] = o >= 0 ? src[o + (int64_t)f * TR] : E(0);
+    }
+}
+
 __global__ void k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
     count_launch(launches);
+    __shared__ int64_t s_src[128];
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
-    int64_t total = 0;
+    int64_t total = 0, tiles = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
+        if (nd.layout >= 2) {
+            tiles += (nd.st->copy_R + nd.layout - 1) / nd.layout;
+            continue;
+        }
         const int es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2;
         total += (int64_t)nd.st->copy_R * (nd.N * es / 16);
     }
@@ -389,6 +417,7 @@ __global__ void k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned
         int n = 0;
         int es = 4, pieces = 1;
         for (; n < nnets; ++n) {
+            if (nets[n].layout >= 2) continue;
             es = nets[n].prec == COSPDNN_PREC_FP32 ? 4 : 2;
             pieces = nets[n].N * es / 16;
             const int64_t cnt = (int64_t)nets[n].st->copy_R * pieces;
@@ -401,8 +430,21 @@ __global__ void k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned
         const int p = nd.cmap[q];
         const char *src = (const char *)nd.act[ib ^ 1];
         char *dst = (char *)nd.act[ib];
-        const uint4 v = *reinterpret_cast<const uint4 *>(src + act_index(nd.tiled, N, p, f) * es);
-        *reinterpret_cast<uint4 *>(dst + act_index(nd.tiled, N, q, f) * es) = v;
+        const uint4 v = *reinterpret_cast<const uint4 *>(src + act_index(nd.layout, N, p, f) * es);
+        *reinterpret_cast<uint4 *>(dst + act_index(nd.layout, N, q, f) * es) = v;
+    }
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        int64_t u = t;
+        int n = 0;
+        for (; n < nnets; ++n) {
+            const NetDev &nd = nets[n];
+            if (nd.layout < 2) continue;
+            const int64_t cnt = (nd.st->copy_R + nd.layout - 1) / nd.layout;
+            if (u < cnt) break;
+            u -= cnt;
+        }
+        if (nets[n].prec == COSPDNN_PREC_FP32) copy_tile<uint32_t>(nets[n], (int)u, s_src);
+        else copy_tile<uint16_t>(nets[n], (int)u, s_src);
     }
 }
 

@@ -76,3 +76,27 @@ def make_half_block_net(neuron, layers, rows, seed=1, dlo=0.1, dhi=0.3, bias=-0.
     csc = [half_block_layer(neuron, seed, 0, l) for l in range(layers)]
     y0 = po.input_binary(seed, 0, rows, neuron, dlo, dhi)
     return csc, y0, np.float32(bias)
+
+
+def random_layer(neuron, seed, layer, kmin=12, kmax=44, wlo=0.02, whi=0.12, neg=0.1):
+    """Unstructured weights: column j has U[kmin, kmax] distinct random inputs
+    (so the per-column entry counts differ), values multiples of 1/256 in
+    [wlo, whi], a fraction `neg` of them negated."""
+    rng = np.random.default_rng(seed * 7919 + layer)
+    colptr = np.zeros(neuron + 1, np.int32)
+    rows, vals = [], []
+    for j in range(neuron):
+        k = int(rng.integers(kmin, kmax + 1))
+        r = np.sort(rng.choice(neuron, size=k, replace=False)).astype(np.int32)
+        v = np.round(rng.uniform(wlo, whi, size=k) * 256) / 256
+        v[rng.random(k) < neg] *= -1
+        rows.append(r)
+        vals.append(v.astype(np.float32))
+        colptr[j + 1] = colptr[j] + k
+    return colptr, np.concatenate(rows), np.concatenate(vals)
+
+
+def make_random_net(neuron, layers, rows, seed=1, dlo=0.2, dhi=0.4, bias=-0.2, **kw):
+    csc = [random_layer(neuron, seed, l, **kw) for l in range(layers)]
+    y0 = po.input_binary(seed, 0, rows, neuron, dlo, dhi)
+    return csc, y0, np.float32(bias)

@@ -147,3 +147,65 @@ def test_engine_tcgen05_layer_values_match_cuda_core(cs):
     r_cc = run_engine(cs, [(csc, y0, b)], 1, 1)[0]
     np.testing.assert_array_equal(r_tc["categories"], r_cc["categories"])
     assert np.abs(r_tc["final"] - r_cc["final"]).max() <= 0.125
+
+
+# Row-tile heights of the CUDA-core tile kernel (tile = N x TR values in at
+# most 200 KB of shared memory): each case exercises a different number of
+# lanes per output (G) and outputs per quarter warp (P = 8/G).
+@pytest.mark.parametrize("n,prec", [(512, 1), (1000, 1), (2048, 2), (3000, 1), (8192, 1),
+                                    (512, 0), (1000, 0), (4096, 0)])
+def test_engine_cc_tile_shapes(cs, n, prec):
+    from netgen import make_random_net
+    csc, y0, b = make_random_net(n, 5, 333, seed=23)
+    ref = oracle_run(csc, y0, b, want_final=True)
+    res = run_engine(cs, [(csc, y0, b)], prec, 1)[0]
+    check_parity(res, ref, 5)
+    if len(ref["categories"]):
+        tol = {0: 1e-3, 1: 0.25, 2: 2.0}[prec]
+        assert np.abs(res["final"] - ref["final"][ref["categories"]]).max() <= tol
+
+
+@pytest.mark.parametrize("n,prec", [(2048, 1), (4096, 2), (8192, 1), (4096, 0)])
+def test_engine_cc_random_weights_sustained(cs, n, prec):
+    """Unequal entry counts per output (12..44): zero-weight padding and the
+    bank-conflict-free entry order with uneven residue loads; rows pruned in
+    the middle layers exercise the row-tile compaction copy."""
+    from netgen import make_random_net
+    csc, y0, b = make_random_net(n, 8, 700, seed=29)
+    ref = oracle_run(csc, y0, b)
+    assert ref["alive"][0] > 0
+    res = run_engine(cs, [(csc, y0, b)], prec, 1)[0]
+    check_parity(res, ref, 8)
+
+
+def test_engine_row_major_gather_kernel_wide_fp32(cs):
+    """FP32 rows of 16384 features do not fit a 16-byte row tile in shared
+    memory: the net runs on the row-major gather kernel."""
+    csc, y0, b = make_net(16384, 4, 200, seed=31, dlo=0.2, dhi=0.4)
+    ref = oracle_run(csc, y0, b)
+    res = run_engine(cs, [(csc, y0, b)], 0, 1)[0]
+    check_parity(res, ref, 4)
+
+
+def test_engine_mixed_kernels_one_graph(cs):
+    """Row-tile, row-major and tcgen05 nets advance in the same graph."""
+    from netgen import make_random_net
+    nets = [make_random_net(2048, 6, 500, seed=37),
+            make_net(16384, 3, 150, seed=37, net=1, dlo=0.2, dhi=0.4),
+            make_net(1024, 7, 400, seed=37, net=2, dlo=0.2, dhi=0.4)]
+    refs = [oracle_run(*n) for n in nets]
+    eng = cs.Engine(0)
+    ids = []
+    for (csc, y0, b), prec, kern in zip(nets, (1, 0, 1), (1, 1, 2)):
+        nid = eng.add_net(y0.shape[1], len(csc), y0.shape[0], float(b), 1e-5, prec, kern)
+        for l, (cp, ri, vv) in enumerate(csc):
+            eng.set_layer_csc(nid, l, cp, ri, vv)
+        ids.append(nid)
+    eng.build()
+    for nid, (_, y0, _) in zip(ids, nets):
+        eng.set_input(nid, y0)
+    eng.run()
+    res = [eng.result(nid) for nid in ids]
+    eng.close()
+    for r, f, n in zip(res, refs, nets):
+        check_parity(r, f, len(n[0]))
