@@ -4,8 +4,9 @@
 // Activations of these nets are stored in row tiles of TR rows, feature-major
 // inside a tile (act_index layout TR), so one tile is a contiguous block of
 // N*TR values and the TR values of one input feature are 16*G adjacent bytes
-// (G = TR*elem/16 >= 1).  A CTA (one per SM, 16 warps) copies a whole tile
-// into shared memory, then computes every output of it: a group of G lanes
+// (G = TR*elem/16 >= 1).  A CTA (two of 8 warps per SM when the tile fits
+// 96 KB, else one of 16 warps) copies a whole tile into shared memory, then
+// computes every output of it: a group of G lanes
 // owns one output j, lane c of the group owns rows c*V..c*V+V-1 of the tile
 // (V = 16 bytes of values: 8 for 16-bit types, 4 for FP32), and for each of
 // the output's entries (input i, weight w) the lane reads the 16 bytes of
@@ -30,15 +31,18 @@
 // Small layers are split into output slices so that the grid stays busy.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "cc_layer.cuh"
 
 namespace cospdnn {
 namespace {
 
-constexpr int kCcThreads = 512;
-constexpr int kCcWarps = kCcThreads / 32;
-constexpr size_t kCcTileBudget = 200 * 1024;  // shared memory for one tile
+// Two CTAs of 256 threads per SM when the tile fits half of shared memory
+// (one CTA stages its next tile while the other computes), else one CTA of
+// 512 threads with a tile of up to 200 KB.
+constexpr size_t kCcPairBudget = 96 * 1024;
+constexpr size_t kCcTileBudget = 200 * 1024;
 constexpr int kCcMaxTR = 128;
 
 template <typename T>
@@ -66,14 +70,14 @@ __device__ __forceinline__ uint4 lds128(uint32_t addr) {
     return v;
 }
 
-// a0 += w * y.lo, a1 += w * y.hi with w = the high half of `ent`; one
+// a0 += w * y.lo, a1 += w * y.hi with w = the low half of `ent`; one
 // rounding each, identical to fmaf on the widened operands.
 __device__ __forceinline__ void fma2(float &a0, float &a1, uint32_t ent, uint32_t y, __half) {
     asm("{\n\t.reg .b16 wl, wh, y0, y1;\n\t"
         "mov.b32 {wl, wh}, %2;\n\t"
         "mov.b32 {y0, y1}, %3;\n\t"
-        "fma.rn.f32.f16 %0, wh, y0, %0;\n\t"
-        "fma.rn.f32.f16 %1, wh, y1, %1;\n\t}"
+        "fma.rn.f32.f16 %0, wl, y0, %0;\n\t"
+        "fma.rn.f32.f16 %1, wl, y1, %1;\n\t}"
         : "+f"(a0), "+f"(a1)
         : "r"(ent), "r"(y));
 }
@@ -81,52 +85,52 @@ __device__ __forceinline__ void fma2(float &a0, float &a1, uint32_t ent, uint32_
     asm("{\n\t.reg .b16 wl, wh, y0, y1;\n\t"
         "mov.b32 {wl, wh}, %2;\n\t"
         "mov.b32 {y0, y1}, %3;\n\t"
-        "fma.rn.f32.bf16 %0, wh, y0, %0;\n\t"
-        "fma.rn.f32.bf16 %1, wh, y1, %1;\n\t}"
+        "fma.rn.f32.bf16 %0, wl, y0, %0;\n\t"
+        "fma.rn.f32.bf16 %1, wl, y1, %1;\n\t}"
         : "+f"(a0), "+f"(a1)
         : "r"(ent), "r"(y));
 }
 
-// One block of 16 entries into the V accumulators.
+// V FMAs of one entry on one 16-byte shared load (V rows of one input).
 template <typename T>
-__device__ __forceinline__ void cc_block(float *acc, const uint4 *q, uint32_t sbase, int lgs) {
+__device__ __forceinline__ void cc_entry(float *acc, uint32_t w, uint32_t addr) {
+    const uint4 y = lds128(addr);
     if constexpr (sizeof(T) == 4) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const uint4 e = q[i];
-            const uint4 y0 = lds128(sbase + (e.x << lgs));
-            const uint4 y1 = lds128(sbase + (e.z << lgs));
-            const float w0 = __uint_as_float(e.y), w1 = __uint_as_float(e.w);
-            acc[0] = fmaf(w0, __uint_as_float(y0.x), acc[0]);
-            acc[1] = fmaf(w0, __uint_as_float(y0.y), acc[1]);
-            acc[2] = fmaf(w0, __uint_as_float(y0.z), acc[2]);
-            acc[3] = fmaf(w0, __uint_as_float(y0.w), acc[3]);
-            acc[0] = fmaf(w1, __uint_as_float(y1.x), acc[0]);
-            acc[1] = fmaf(w1, __uint_as_float(y1.y), acc[1]);
-            acc[2] = fmaf(w1, __uint_as_float(y1.z), acc[2]);
-            acc[3] = fmaf(w1, __uint_as_float(y1.w), acc[3]);
-        }
+        const float wf = __uint_as_float(w);
+        acc[0] = fmaf(wf, __uint_as_float(y.x), acc[0]);
+        acc[1] = fmaf(wf, __uint_as_float(y.y), acc[1]);
+        acc[2] = fmaf(wf, __uint_as_float(y.z), acc[2]);
+        acc[3] = fmaf(wf, __uint_as_float(y.w), acc[3]);
     } else {
+        fma2(acc[0], acc[1], w, y.x, T());
+        fma2(acc[2], acc[3], w, y.y, T());
+        fma2(acc[4], acc[5], w, y.z, T());
+        fma2(acc[6], acc[7], w, y.w, T());
+    }
+}
+
+// One block of four 16-byte groups of entries into the V accumulators: 16
+// entries of a 16-bit net ((column << 16) | weight bits, 4 per group) or 8 of
+// an FP32 net ({column, weight bits}, 2 per group); column = the input's
+// 16-byte column in the tile (input * G).
+template <typename T>
+__device__ __forceinline__ void cc_block(float *acc, const uint4 *q, uint32_t sbase) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 4; ++i) {
+        if constexpr (sizeof(T) == 4) {
+            cc_entry<T>(acc, q[i].y, sbase + (q[i].x << 4));
+            cc_entry<T>(acc, q[i].w, sbase + (q[i].z << 4));
+        } else {
             const uint32_t ent[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const uint4 y = lds128(sbase + ((ent[e] & 0xFFFFu) << lgs));
-                fma2(acc[0], acc[1], ent[e], y.x, T());
-                fma2(acc[2], acc[3], ent[e], y.y, T());
-                fma2(acc[4], acc[5], ent[e], y.z, T());
-                fma2(acc[6], acc[7], ent[e], y.w, T());
-            }
+            for (int e = 0; e < 4; ++e) cc_entry<T>(acc, ent[e], sbase + ((ent[e] >> 16) << 4));
         }
     }
 }
 
-template <typename T>
 __device__ __forceinline__ void cc_load(uint4 *q, const uint4 *__restrict__ W, int N, int j, int b) {
-    constexpr int NQ = 16 / cc_traits<T>::EPV;
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) q[i] = __ldg(W + (int64_t)(b * NQ + i) * N + j);
+    for (int i = 0; i < 4; ++i) q[i] = __ldg(W + (int64_t)(b * 4 + i) * N + j);
 }
 
 __device__ __forceinline__ bool cc_net(const NetDev &nd, int prec) {
@@ -136,10 +140,10 @@ __device__ __forceinline__ bool cc_net(const NetDev &nd, int prec) {
 // Output slices per tile: the split (1, 2, 4, ... up to one CTA round of
 // outputs per slice) whose last wave of items wastes the least of the grid,
 // charging each extra slice for re-reading the tile.
-__device__ __forceinline__ int cc_slices(const NetDev &nd, int es, int grid) {
-    const int TR = nd.layout;
+__device__ __forceinline__ int cc_slices(const NetDev &nd, int grid, int warps) {
+    const int TR = nd.layout, es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2;
     const int ntiles = (nd.st->R + TR - 1) / TR;
-    const int step = kCcWarps * (32 / (TR * es / 16));
+    const int step = warps * (32 / (TR * es / 16));
     const int rounds = (nd.N + step - 1) / step;
     int best = 1;
     double best_cost = 1e30;
@@ -159,12 +163,12 @@ struct CcItem {
     int net, tile, slice, slices;
 };
 
-__device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int prec, int es, int grid, int64_t u,
+__device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int prec, int grid, int warps, int64_t u,
                                           CcItem &it) {
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (!cc_net(nd, prec)) continue;
-        const int S = cc_slices(nd, es, grid);
+        const int S = cc_slices(nd, grid, warps);
         const int64_t cnt = (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * S;
         if (u < cnt) {
             it.net = n;
@@ -178,54 +182,96 @@ __device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int pre
     return false;
 }
 
+// Bound on |stored - clamped| for a value c in [0, 32] stored in the compute
+// type: half an ulp, at most 2^-11 c + 2^-25 (FP16; 2^-25 covers the
+// subnormal range) or 2^-8 c + 2^-126 (BF16, more than its subnormal half
+// spacing); 0 for FP32.
 template <typename T>
-__global__ void __launch_bounds__(kCcThreads, 1)
+__device__ __forceinline__ float store_error(float c) {
+    if constexpr (sizeof(T) == 4) return 0.0f;
+    else if constexpr (std::is_same<T, __half>::value) return __fmaf_ru(c, 4.8828125e-04f, 2.98023224e-08f);
+    else return __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
+}
+
+// Row statistics from the row's max pre-activation zm and its error bound ez:
+//   max output  = the stored value of clamp(zm) (rounding is monotone, so
+//                 this is the max of the stored outputs);
+//   output error: outputs with z <= -ez are 0 in both recurrences and those
+//                 with z >= 32 + ez are 32 in both; any other output is
+//                 within ez of the exact clamp plus its storage rounding, and
+//                 is at most clamp(zm): bound ez + store_error(clamp(zm)) when
+//                 zm > -ez, else 0.
+template <typename T>
+__device__ __forceinline__ void row_stats(float zm, float ez, float &emax, float &ymax) {
+    const float c = clamp32(zm);
+    ymax = act_traits<T>::to_f(act_traits<T>::from_f(c));
+    emax = zm > -ez ? __fadd_ru(ez, store_error<T>(c)) : 0.0f;
+}
+
+// Bias, clamp, store of V accumulators as one 16-byte piece; max z per row.
+template <typename T>
+__device__ __forceinline__ void cc_store(float *acc, float *zmax, float bias, T *dst) {
+    constexpr int V = cc_traits<T>::V;
+    __align__(16) T ov[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const float z = acc[v] + bias;
+        zmax[v] = fmaxf(zmax[v], z);
+        ov[v] = act_traits<T>::from_f(clamp32(z));
+        acc[v] = 0.0f;
+    }
+    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(ov);
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
     k_layer_cc(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
     count_launch(launches);
-    using tr = cc_traits<T>;
-    constexpr int ES = (int)sizeof(T), V = tr::V, NQ = 16 / tr::EPV;
+    constexpr int ES = (int)sizeof(T), V = cc_traits<T>::V, kWarps = NT / 32;
+    constexpr int EB = 4 * cc_traits<T>::EPV;  // entries per block
     extern __shared__ uint4 cc_smem[];
-    __shared__ uint32_t s_stat[kCcMaxTR * 3];
+    __shared__ uint32_t s_zmax[kCcMaxTR];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grid = (int)gridDim.x;
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (!cc_net(nd, prec)) continue;
-        total += (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * cc_slices(nd, ES, grid);
+        total += (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * cc_slices(nd, grid, kWarps);
     }
     for (int64_t item = blockIdx.x; item < total; item += grid) {
         CcItem it;
-        cc_locate(nets, nnets, prec, ES, grid, item, it);
+        cc_locate(nets, nnets, prec, grid, kWarps, item, it);
         const NetDev &nd = nets[it.net];
         const int N = nd.N, TR = nd.layout, l = nd.st->layer, R = nd.st->R, par = l & 1, ib = nd.st->in_buf;
         const LayerDev &lw = nd.layers[l];
         const T *in = (const T *)(l == 0 ? nd.y0 : nd.act[ib]);
         T *out = (T *)nd.act[ib ^ 1];
-        const int G = TR * ES / 16, lg = __ffs(G) - 1, lgs = __ffs(TR * ES) - 1;
-        const int opw = 32 >> lg;  // outputs per warp and round
+        const int G = TR * ES / 16, lg = __ffs(G) - 1;  // lanes per output
+        const int opw = 32 >> lg;                        // outputs per warp and round
         const int c = lane & (G - 1), o = lane >> lg;
 
-        // ---- stage the tile (and the statistics) in shared memory
-        __syncthreads();  // the previous item is done with both
+        // ---- stage the tile in shared memory
+        __syncthreads();  // the previous item is done with the tile and s_zmax
         {
             const uint4 *src = reinterpret_cast<const uint4 *>(in + (int64_t)it.tile * N * TR);
-            const int nvec = N * G;
+            const int nvec = N * TR * ES / 16;
             int i = threadIdx.x;
-            for (; i + 7 * kCcThreads < nvec; i += 8 * kCcThreads) {
+            for (; i + 7 * NT < nvec; i += 8 * NT) {
                 uint4 v[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) v[k] = __ldg(src + i + k * kCcThreads);
+                for (int k = 0; k < 8; ++k) v[k] = __ldg(src + i + k * NT);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) cc_smem[i + k * kCcThreads] = v[k];
+                for (int k = 0; k < 8; ++k) cc_smem[i + k * NT] = v[k];
             }
-            for (; i < nvec; i += kCcThreads) cc_smem[i] = __ldg(src + i);
-            for (int r = threadIdx.x; r < TR * 3; r += kCcThreads) s_stat[r] = 0u;
+            for (; i < nvec; i += NT) cc_smem[i] = __ldg(src + i);
+            for (int r = threadIdx.x; r < TR; r += NT) s_zmax[r] = 0u;
         }
         if (threadIdx.x == 0 && item + grid < total) {
             // the next tile of this CTA into L2 while this one is computed
             CcItem nx;
-            if (cc_locate(nets, nnets, prec, ES, grid, item + grid, nx) && (nx.net != it.net || nx.tile != it.tile)) {
+            if (cc_locate(nets, nnets, prec, grid, kWarps, item + grid, nx) &&
+                (nx.net != it.net || nx.tile != it.tile)) {
                 const NetDev &nn = nets[nx.net];
                 const T *nin = (const T *)(nn.st->layer == 0 ? nn.y0 : nn.act[nn.st->in_buf]);
                 const uint32_t bytes = (uint32_t)((size_t)nn.N * nn.layout * ES);
@@ -236,93 +282,78 @@ __global__ void __launch_bounds__(kCcThreads, 1)
         }
         __syncthreads();
 
-        // ---- per-row error bounds of this lane's rows
-        const double steps = fast_steps(nd, lw);
-        const int row0 = it.tile * TR + c * V;
-        float ez[V], zmax[V], emax[V], ymax[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const int p = row0 + v;
-            ez[v] = p < R ? z_error_bound(nd.err[par][p], nd.mx[par][p], lw.S, lw.dW, nd.bias, steps) : 0.0f;
-            zmax[v] = -INFINITY;
-            emax[v] = 0.0f;
-            ymax[v] = 0.0f;
-        }
-
-        // ---- outputs of this slice
-        const int step = kCcWarps * opw;
+        // ---- outputs of this slice: step s = (output jc, block bc), entries
+        // of step s+2 loaded while step s is computed (three buffers)
+        const int step = kWarps * opw;
         const int rounds = (N + step - 1) / step;
         const int j_lo = (it.slice * rounds / it.slices) * step;
         const int j_hi = min(N, ((it.slice + 1) * rounds / it.slices) * step);
-        const int nb = lw.cc_k / 16;
+        const int nb = lw.cc_k / EB;
         const uint4 *__restrict__ W = lw.cc_w;
         const uint32_t sbase = smem_u32(cc_smem) + c * 16;
         const float bias = nd.bias;
-        int j = j_lo + warp * opw + o, b = 0;
-        bool have = j < j_hi;
-        uint4 cur[NQ], nxt[NQ];
-        if (have) cc_load<T>(cur, W, N, j, 0);
-        float acc[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = 0.0f;
-        while (have) {
-            int jn = j, bn = b + 1;
-            if (bn == nb) {
-                bn = 0;
-                jn += step;
-            }
-            const bool hn = jn < j_hi;
-            if (hn) cc_load<T>(nxt, W, N, jn, bn);
-            cc_block<T>(acc, cur, sbase, lgs);
-            if (bn == 0) {
-                __align__(16) T ov[V];
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float z = acc[v] + bias;
-                    const float cl = clamp32(z);
-                    const T ys = act_traits<T>::from_f(cl);
-                    const float yf = act_traits<T>::to_f(ys);
-                    ov[v] = ys;
-                    zmax[v] = fmaxf(zmax[v], z);
-                    ymax[v] = fmaxf(ymax[v], yf);
-                    if (z > -ez[v] && z < 32.0f + ez[v]) emax[v] = fmaxf(emax[v], __fadd_ru(ez[v], fabsf(yf - cl)));
-                    acc[v] = 0.0f;
-                }
-                *reinterpret_cast<uint4 *>(out + ((int64_t)it.tile * N + j) * TR + c * V) =
-                    *reinterpret_cast<const uint4 *>(ov);
-            }
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) cur[i] = nxt[i];
-            j = jn;
-            b = bn;
-            have = hn;
-        }
-
-        // ---- row statistics: lanes of equal c, then warps, then global
+        const int j0 = j_lo + warp * opw + o;
+        const int nout = j0 < j_hi ? (j_hi - j0 + step - 1) / step : 0;
+        const int nsteps = nout * nb;
+        float acc[V], zmax[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-            for (int off = G; off < 32; off <<= 1) {
-                zmax[v] = fmaxf(zmax[v], __shfl_xor_sync(0xffffffffu, zmax[v], off));
-                emax[v] = fmaxf(emax[v], __shfl_xor_sync(0xffffffffu, emax[v], off));
-                ymax[v] = fmaxf(ymax[v], __shfl_xor_sync(0xffffffffu, ymax[v], off));
-            }
+            acc[v] = 0.0f;
+            zmax[v] = -INFINITY;
         }
+        int jl = j0, bl = 0, jc = j0, bc = 0;
+        uint4 qa[4], qb[4], qc[4];
+        auto next_load = [&](uint4 *q) {
+            cc_load(q, W, N, jl, bl);
+            if (++bl == nb) {
+                bl = 0;
+                jl += step;
+            }
+        };
+        auto finish_step = [&]() {
+            if (++bc == nb) {
+                cc_store<T>(acc, zmax, bias, out + ((int64_t)it.tile * N + jc) * TR + c * V);
+                bc = 0;
+                jc += step;
+            }
+        };
+        if (nsteps > 0) next_load(qa);
+        if (nsteps > 1) next_load(qb);
+        for (int s = 0; s < nsteps; s += 3) {
+            if (s + 2 < nsteps) next_load(qc);
+            cc_block<T>(acc, qa, sbase);
+            finish_step();
+            if (s + 1 >= nsteps) break;
+            if (s + 3 < nsteps) next_load(qa);
+            cc_block<T>(acc, qb, sbase);
+            finish_step();
+            if (s + 2 >= nsteps) break;
+            if (s + 4 < nsteps) next_load(qb);
+            cc_block<T>(acc, qc, sbase);
+            finish_step();
+        }
+
+        // ---- row statistics: max z over lanes of equal c, then warps, then
+        // the row's error bound, max output and output error
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            for (int off = G; off < 32; off <<= 1) zmax[v] = fmaxf(zmax[v], __shfl_xor_sync(0xffffffffu, zmax[v], off));
         if (o == 0) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const int r = c * V + v;
-                atomicMax(&s_stat[3 * r], f2ord(zmax[v]));
-                atomicMax(&s_stat[3 * r + 1], __float_as_uint(emax[v]));
-                atomicMax(&s_stat[3 * r + 2], __float_as_uint(ymax[v]));
-            }
+            for (int v = 0; v < V; ++v) atomicMax(&s_zmax[c * V + v], f2ord(zmax[v]));
         }
         __syncthreads();
-        for (int r = threadIdx.x; r < TR; r += kCcThreads) {
+        const double steps = fast_steps(nd, lw);
+        for (int r = threadIdx.x; r < TR; r += NT) {
             const int p = it.tile * TR + r;
             if (p < R) {
-                atomicMax(&nd.stat[3 * p], s_stat[3 * r]);
-                atomicMax(&nd.stat[3 * p + 1], s_stat[3 * r + 1]);
-                atomicMax(&nd.stat[3 * p + 2], s_stat[3 * r + 2]);
+                const float zm = ord2f(s_zmax[r]);
+                const float ez = z_error_bound(nd.err[par][p], nd.mx[par][p], lw.S, lw.dW, bias, steps);
+                float em, ym;
+                row_stats<T>(zm, ez, em, ym);
+                atomicMax(&nd.stat[3 * p], s_zmax[r]);
+                atomicMax(&nd.stat[3 * p + 1], __float_as_uint(em));
+                atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));
             }
         }
     }
@@ -396,8 +427,9 @@ int colour_group(int P, const std::vector<int> &eu, const std::vector<int> &es, 
 int cc_tile_rows(int N, int prec) {
     const int es = prec == COSPDNN_PREC_FP32 ? 4 : 2;
     if (N > 65536) return 0;  // 16-bit input indices
-    for (int TR = kCcMaxTR; TR >= 2; TR >>= 1)
-        if (TR * es >= 16 && (size_t)N * TR * es <= kCcTileBudget) return TR;
+    for (size_t budget : {kCcPairBudget, kCcTileBudget})
+        for (int TR = kCcMaxTR; TR >= 2; TR >>= 1)
+            if (TR * es >= 16 && (size_t)N * TR * es <= budget) return TR;
     return 0;
 }
 
@@ -405,47 +437,58 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
                      const std::vector<float> &vals, int N, int prec, int TR, LayerDev &ld,
                      std::vector<void *> &owned) {
     const int es = prec == COSPDNN_PREC_FP32 ? 4 : 2;
-    const int G = TR * es / 16;
-    const int P = G >= 8 ? 1 : 8 / G;  // outputs per quarter warp
-    CSP_CHECK(G >= 1 && N % P == 0, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: bad tile");
+    const int colw = TR * es / 16;     // 16-byte columns per feature = lanes per output
+    const int B = colw >= 8 ? 1 : 8 / colw;  // outputs per quarter warp
+    const int P = B;                         // residues that must differ
+    CSP_CHECK(colw >= 1 && N % B == 0, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: bad tile");
+    CSP_CHECK((size_t)N * colw <= 65536, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: tile too large");
+    // groups of outputs whose entries must have distinct residues mod P at
+    // every step: the B outputs of a quarter warp
+    std::vector<std::vector<int>> groups;
+    for (int g0 = 0; g0 < N; g0 += B) {
+        groups.emplace_back();
+        for (int u = 0; u < B; ++u) groups.back().push_back(g0 + u);
+    }
     // per output: the entries (CSC positions, -1 = padding) in step order
     std::vector<std::vector<int>> order(N);
-    std::vector<std::vector<int>> pad_idx(N);
     int Kmax = 1;
     std::vector<int> eu, esl, ep, colour;
-    for (int g0 = 0; g0 < N; g0 += P) {
+    for (const auto &grp : groups) {
         eu.clear();
         esl.clear();
         ep.clear();
-        for (int u = 0; u < P; ++u)
-            for (int p = colptr[g0 + u]; p < colptr[g0 + u + 1]; ++p) {
+        for (int u = 0; u < (int)grp.size(); ++u)
+            for (int p = colptr[grp[u]]; p < colptr[grp[u] + 1]; ++p) {
                 eu.push_back(u);
                 esl.push_back(rowidx[p] % P);
                 ep.push_back(p);
             }
-        const int D = P == 1 ? (int)eu.size() : colour_group(P, eu, esl, colour);
-        Kmax = std::max(Kmax, D);
-        for (int u = 0; u < P; ++u) order[g0 + u].assign(D, -1);
+        const int D = P == 1 ? (int)ep.size() : colour_group(P, eu, esl, colour);
+        for (int u = 0; u < (int)grp.size(); ++u) order[grp[u]].assign(D, -1);
         if (P == 1) {
-            for (int e = 0; e < (int)ep.size(); ++e) order[g0][e] = ep[e];
+            // no constraint: each output's entries in ascending input order
+            for (int u = 0; u < (int)grp.size(); ++u) {
+                const int j = grp[u], k = colptr[j + 1] - colptr[j];
+                order[j].assign(k, -1);
+                for (int t = 0; t < k; ++t) order[j][t] = colptr[j] + t;
+                Kmax = std::max(Kmax, k);
+            }
         } else {
-            for (int e = 0; e < (int)ep.size(); ++e) order[g0 + eu[e]][colour[e]] = ep[e];
+            Kmax = std::max(Kmax, D);
+            for (int e = 0; e < (int)ep.size(); ++e) order[grp[eu[e]]][colour[e]] = ep[e];
         }
     }
     const int Kc = (Kmax + 15) / 16 * 16;
-    // padding at step t of a group: a residue unused by the group at t
-    const int epv = es == 4 ? 2 : 4;
+    const int epv = es == 4 ? 2 : 4;  // entries per 16-byte group
     const size_t ngroups = (size_t)Kc / epv;
     std::vector<uint32_t> packed(ngroups * N * 4, 0u);
-    for (int g0 = 0; g0 < N; g0 += P) {
+    for (const auto &grp : groups) {
         for (int t = 0; t < Kc; ++t) {
+            // padding at step t: a residue unused by the group at t
             uint32_t used = 0;
-            for (int u = 0; u < P; ++u) {
-                const auto &ord = order[g0 + u];
-                if (t < (int)ord.size() && ord[t] >= 0) used |= 1u << (rowidx[ord[t]] % P);
-            }
-            for (int u = 0; u < P; ++u) {
-                const int j = g0 + u;
+            for (int j : grp)
+                if (t < (int)order[j].size() && order[j][t] >= 0) used |= 1u << (rowidx[order[j][t]] % P);
+            for (int j : grp) {
                 const auto &ord = order[j];
                 int idx;
                 float w;
@@ -461,17 +504,18 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
                     idx = r;  // residue r (N >= P)
                     w = 0.0f;
                 }
-                const size_t grp = (size_t)(t / epv), slot = (size_t)(t % epv);
-                uint32_t *dst = &packed[(grp * N + j) * 4];
+                const size_t g = (size_t)(t / epv), slot = (size_t)(t % epv);
+                uint32_t *dst = &packed[(g * N + j) * 4];
+                const uint32_t col = (uint32_t)idx * colw;  // first 16-byte column of the input
                 if (es == 4) {
-                    dst[2 * slot] = (uint32_t)idx;
+                    dst[2 * slot] = col;
                     uint32_t wb;
                     std::memcpy(&wb, &w, 4);
                     dst[2 * slot + 1] = wb;
                 } else {
                     const uint32_t wb = prec == COSPDNN_PREC_FP16 ? weight_bits<__half>(w)
                                                                   : weight_bits<__nv_bfloat16>(w);
-                    dst[slot] = (uint32_t)idx | (wb << 16);
+                    dst[slot] = (col << 16) | wb;
                 }
             }
         }
@@ -487,12 +531,15 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
 
 int cc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms,
                   size_t max_tile_bytes) {
-    k.fn = prec == COSPDNN_PREC_FP32   ? (void *)k_layer_cc<float>
-         : prec == COSPDNN_PREC_FP16 ? (void *)k_layer_cc<__half>
-                                     : (void *)k_layer_cc<__nv_bfloat16>;
+    using F = void (*)(const NetDev *, int, int, unsigned long long *);
+    static const F fns[3][2] = {{k_layer_cc<float, 512>, k_layer_cc<float, 256>},
+                                {k_layer_cc<__half, 512>, k_layer_cc<__half, 256>},
+                                {k_layer_cc<__nv_bfloat16, 512>, k_layer_cc<__nv_bfloat16, 256>}};
+    const bool pair = max_tile_bytes <= kCcPairBudget;
+    k.fn = (void *)fns[prec][pair ? 1 : 0];
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_tile_bytes));
-    k.grid = dim3(sms);  // one CTA per SM (the tile fills shared memory)
-    k.block = dim3(kCcThreads);
+    k.grid = dim3(pair ? 2 * sms : sms);
+    k.block = dim3(pair ? 256 : 512);
     k.smem = max_tile_bytes;
     k.arg(nets).arg(nnets).arg(prec).arg(launches);
     return COSPDNN_OK;

@@ -46,6 +46,90 @@ __global__ void k_convert_input(const void *__restrict__ src, int rows, int N, i
     }
 }
 
+// Integer inputs (bytes or bits) into row tiles (layout TR >= 2): one thread
+// per (tile, run of up to 8 rows, 8 features); each feature's run of rows is
+// written as one contiguous piece.  Values 0..255 are exact in every compute
+// type, so the per-row error is 0 (k_row_max fills it and the row max).
+template <typename T, int FMT>
+__global__ void k_convert_tile(const uint8_t *__restrict__ src, int rows, int N, int TR, T *__restrict__ y0) {
+    const int RC = TR < 8 ? TR : 8, nrc = TR / RC, nfb = N / 8;
+    const int64_t ntiles = (rows + TR - 1) / TR;
+    const int64_t total = ntiles * nrc * nfb;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (int64_t)gridDim.x * blockDim.x) {
+        const int fb = (int)(u % nfb);
+        const int64_t rest = u / nfb;
+        const int rc = (int)(rest % nrc);
+        const int64_t t = rest / nrc;
+        uint8_t v[8][8];  // [row][feature]
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int64_t row = t * TR + rc * RC + r;
+            uint2 b = make_uint2(0u, 0u);
+            if (r < RC && row < rows) {
+                if (FMT == COSPDNN_INPUT_U8) {
+                    b = *reinterpret_cast<const uint2 *>(src + row * N + 8 * fb);
+                } else {
+                    const uint32_t bits = src[row * nfb + fb];
+                    // byte k of the pair = bit k of the feature byte
+                    b.x = (bits & 1u) | ((bits >> 1) & 1u) << 8 | ((bits >> 2) & 1u) << 16 | ((bits >> 3) & 1u) << 24;
+                    b.y = ((bits >> 4) & 1u) | ((bits >> 5) & 1u) << 8 | ((bits >> 6) & 1u) << 16 | ((bits >> 7) & 1u) << 24;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[r][k] = (uint8_t)(b.x >> (8 * k));
+                v[r][k + 4] = (uint8_t)(b.y >> (8 * k));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            T *dst = y0 + ((t * N + 8 * fb + k) * TR + rc * RC);
+            __align__(16) T o[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) o[r] = act_traits<T>::from_f((float)v[r][k]);
+            if (RC * (int)sizeof(T) == 16) {
+                *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(o);
+            } else if (RC * (int)sizeof(T) == 32) {
+                reinterpret_cast<uint4 *>(dst)[0] = reinterpret_cast<const uint4 *>(o)[0];
+                reinterpret_cast<uint4 *>(dst)[1] = reinterpret_cast<const uint4 *>(o)[1];
+            } else {
+                for (int r = 0; r < RC; ++r) dst[r] = o[r];
+            }
+        }
+    }
+}
+
+// Per-row max |input| (error 0) of integer inputs: one warp per row.
+template <int FMT>
+__global__ void k_row_max(const uint8_t *__restrict__ src, int rows, int N, float *__restrict__ err0,
+                          float *__restrict__ mx0) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int nb = FMT == COSPDNN_INPUT_U8 ? N : N / 8;  // bytes per row
+    for (int64_t r = w; r < rows; r += nw) {
+        uint32_t m = 0;
+        const uint8_t *row = src + r * nb;
+        if (FMT == COSPDNN_INPUT_U8) {
+            // N is a multiple of 8, so every row starts 8-byte aligned
+            for (int i = lane * 8; i < nb; i += 256) {
+                const uint2 v = *reinterpret_cast<const uint2 *>(row + i);
+                m = max(m, __vmaxu4(v.x, v.y));
+            }
+        } else {
+            for (int i = lane; i < nb; i += 32) m |= row[i];  // rows of N/8 bytes: any alignment
+        }
+        if (FMT == COSPDNN_INPUT_U8) m = max(max(m & 0xFFu, (m >> 8) & 0xFFu), max((m >> 16) & 0xFFu, m >> 24));
+        else m = m ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) {
+            err0[r] = 0.0f;
+            mx0[r] = (float)m;
+        }
+    }
+}
+
 // gather of the final activations (checks only)
 template <typename T>
 __global__ void k_gather_final(const NetDev *__restrict__ nd_p, float *__restrict__ out, int64_t max_rows) {
@@ -198,8 +282,9 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
 
 // Precisions of the nets on each layer kernel.
 struct KernelSets {
-    std::vector<int> plain, cc, tc;
-    size_t cc_tile_bytes = 0;  // largest row tile of the cc nets
+    std::vector<int> plain, tc;
+    // row-tile kernel: precision -> largest row tile of those nets
+    std::vector<std::pair<int, size_t>> cc;
 };
 
 int make_specs(cospdnn_engine *e, const KernelSets &ks) {
@@ -226,9 +311,9 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         k.arg(nets).arg(nn).arg(prec).arg(launches);
         e->layer_specs.push_back(std::move(k));
     }
-    for (int prec : ks.cc) {
+    for (const auto &cc : ks.cc) {
         KSpec k;
-        int rc = cc_layer_spec(k, nets, nn, prec, launches, sms, ks.cc_tile_bytes);
+        int rc = cc_layer_spec(k, nets, nn, cc.first, launches, sms, cc.second);
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
@@ -450,10 +535,16 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         // activation layout: MMA tiles (tcgen05), row tiles (CUDA-core tile
         // kernel) or row-major (CUDA-core gather kernel, rows too wide for a tile)
         n.dev.layout = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? 1 : cc_tile_rows(n.d.neuron, n.d.precision);
-        auto &v = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? ks.tc : n.dev.layout >= 2 ? ks.cc : ks.plain;
-        if (std::find(v.begin(), v.end(), n.d.precision) == v.end()) v.push_back(n.d.precision);
-        if (n.dev.layout >= 2)
-            ks.cc_tile_bytes = std::max(ks.cc_tile_bytes, cc_tile_bytes(n.d.neuron, n.d.precision, n.dev.layout));
+        if (n.dev.layout >= 2) {
+            const int key = n.d.precision;
+            const size_t tb = cc_tile_bytes(n.d.neuron, n.d.precision, n.dev.layout);
+            auto it = std::find_if(ks.cc.begin(), ks.cc.end(), [&](const auto &x) { return x.first == key; });
+            if (it == ks.cc.end()) ks.cc.push_back({key, tb});
+            else it->second = std::max(it->second, tb);
+        } else {
+            auto &v = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? ks.tc : ks.plain;
+            if (std::find(v.begin(), v.end(), n.d.precision) == v.end()) v.push_back(n.d.precision);
+        }
     }
     for (Net &n : e->nets) {
         const int N = n.d.neuron, R = std::max(1, n.d.rows);
@@ -552,7 +643,11 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     const void *src = y0;
     if (!on_device) {
         if (n.staging_bytes < bytes) {
-            if (n.staging) cudaFree(n.staging);
+            if (n.staging) {
+                // the engine owns the old buffer: drop it from the list it frees at destruction
+                e->owned.erase(std::remove(e->owned.begin(), e->owned.end(), n.staging), e->owned.end());
+                cudaFree(n.staging);
+            }
             n.staging = nullptr;
             n.staging_bytes = 0;
             CSP_CUDA(cudaMalloc(&n.staging, bytes));
@@ -577,6 +672,22 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     }
     const int blocks = std::min(65535, (R + 7) / 8);
     float *err0 = (float *)n.dev.err0, *mx0 = (float *)n.dev.mx0;
+    if (n.dev.layout >= 2 && format != COSPDNN_INPUT_F32) {
+        // integer input into row tiles
+        const uint8_t *b = (const uint8_t *)src;
+        const int TR = n.dev.layout;
+        const int64_t units = (int64_t)((R + TR - 1) / TR) * (TR / std::min(TR, 8)) * (N / 8);
+        const int cb = (int)std::min<int64_t>((units + 255) / 256, 148 * 16);
+#define CSP_TILE(T)                                                                                             do {                                                                                                            if (format == COSPDNN_INPUT_U8) k_convert_tile<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)n.dev.y0);         else k_convert_tile<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)n.dev.y0);                } while (0)
+        if (n.d.precision == COSPDNN_PREC_FP32) CSP_TILE(float);
+        else if (n.d.precision == COSPDNN_PREC_FP16) CSP_TILE(__half);
+        else CSP_TILE(__nv_bfloat16);
+#undef CSP_TILE
+        if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
+        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
+        CSP_CUDA(cudaGetLastError());
+        return COSPDNN_OK;
+    }
 #define CSP_CONV(T)                                                                                      \
     do {                                                                                                 \
         T *dst = (T *)n.dev.y0;                                                                          \

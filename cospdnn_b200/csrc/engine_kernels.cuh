@@ -210,10 +210,29 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
     for (int ll = 0; ll <= l; ++ll) {
         const LayerDev &lw = nd.layers[ll];
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            // entries in ascending input order, loads issued 8 ahead of the
+            // (strictly sequential) accumulation
             double acc = 0.0;
-            for (int k = 0; k < lw.K; ++k) {
-                const double yi = y[__ldg(lw.ell_idx + (int64_t)k * N + j)];
-                if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)__ldg(lw.ell_val + (int64_t)k * N + j), yi));
+            const int32_t *ip = lw.ell_idx + j;
+            const float *wp = lw.ell_val + j;
+            int k = 0;
+            for (; k + 8 <= lw.K; k += 8) {
+                int32_t ii[8];
+                float ww[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    ii[t] = __ldg(ip + (int64_t)(k + t) * N);
+                    ww[t] = __ldg(wp + (int64_t)(k + t) * N);
+                }
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const double yi = y[ii[t]];
+                    if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)ww[t], yi));
+                }
+            }
+            for (; k < lw.K; ++k) {
+                const double yi = y[__ldg(ip + (int64_t)k * N)];
+                if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)__ldg(wp + (int64_t)k * N), yi));
             }
             z[j] = clamp32d(__dadd_rn(acc, b));
         }
@@ -302,33 +321,48 @@ __global__ void __launch_bounds__(kCompactThreads)
     __syncthreads();
     if (!s_done) {
         const int l = s_layer, R = s_R, par = l & 1;
-        for (int base = 0; base < R; base += kCompactThreads) {
-            const int p = base + threadIdx.x;
-            const int keep = (p < R && nd.cls[p] == CLS_KEEP) ? 1 : 0;
-            const unsigned m = __ballot_sync(0xffffffffu, keep);
-            if (lane == 31) warp_tot[wid] = __popc(m);
+        constexpr int kRun = 8;  // consecutive rows per thread and pass (stable order)
+        for (int base = 0; base < R; base += kCompactThreads * kRun) {
+            const int p0 = base + threadIdx.x * kRun;
+            uint32_t keep = 0;
+#pragma unroll
+            for (int i = 0; i < kRun; ++i)
+                if (p0 + i < R && nd.cls[p0 + i] == CLS_KEEP) keep |= 1u << i;
+            int v = __popc(keep);
+            // inclusive scan of the per-thread counts over the warp, then the warps
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (lane == 31) warp_tot[wid] = v;
             __syncthreads();
             if (wid == 0) {
-                int v = warp_tot[lane];
+                int w = warp_tot[lane];
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, v, o);
-                    if (lane >= o) v += t;
+                    const int t = __shfl_up_sync(0xffffffffu, w, o);
+                    if (lane >= o) w += t;
                 }
-                warp_tot[lane] = v;
+                warp_tot[lane] = w;
             }
             __syncthreads();
-            if (keep) {
-                const int q = carry + (wid ? warp_tot[wid - 1] : 0) + __popc(m & ((1u << lane) - 1u));
-                nd.cmap[q] = p;
-                nd.orig[par ^ 1][q] = nd.orig[par][p];
-                nd.err[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 1]);
-                nd.mx[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 2]);
-            }
-            if (p < R) {
-                nd.stat[3 * p] = 0u;
-                nd.stat[3 * p + 1] = 0u;
-                nd.stat[3 * p + 2] = 0u;
+            int q = carry + (wid ? warp_tot[wid - 1] : 0) + v - __popc(keep);
+#pragma unroll
+            for (int i = 0; i < kRun; ++i) {
+                const int p = p0 + i;
+                if ((keep >> i) & 1u) {
+                    nd.cmap[q] = p;
+                    nd.orig[par ^ 1][q] = nd.orig[par][p];
+                    nd.err[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 1]);
+                    nd.mx[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 2]);
+                    ++q;
+                }
+                if (p < R) {
+                    nd.stat[3 * p] = 0u;
+                    nd.stat[3 * p + 1] = 0u;
+                    nd.stat[3 * p + 2] = 0u;
+                }
             }
             __syncthreads();
             if (threadIdx.x == 0) carry += warp_tot[kCompactThreads / 32 - 1];

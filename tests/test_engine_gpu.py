@@ -209,3 +209,32 @@ def test_engine_mixed_kernels_one_graph(cs):
     eng.close()
     for r, f, n in zip(res, refs, nets):
         check_parity(r, f, len(n[0]))
+
+
+@pytest.mark.parametrize("n,prec,kernel", [(1000, 1, 1), (4096, 1, 1), (1024, 0, 1), (4096, 2, 2), (16384, 0, 1)])
+def test_engine_input_formats_agree(cs, n, prec, kernel):
+    """Bytes, packed bits (little-endian within a byte) and float32 inputs of
+    the same binary rows give identical results (row tiles, MMA tiles and
+    row-major layouts), equal to the oracle's."""
+    if n & (n - 1):  # XOR masks need a power of two; N/8 odd = unaligned bit rows
+        from netgen import make_random_net
+        csc, y0, b = make_random_net(n, 4, 333, seed=41)
+    else:
+        csc, y0, b = make_net(n, 4, 333, seed=41, dlo=0.2, dhi=0.4)
+    ref = oracle_run(csc, y0, b)
+    bits = np.packbits(y0, axis=1, bitorder="little")
+    eng = cs.Engine(0)
+    nid = eng.add_net(n, 4, y0.shape[0], float(b), 1e-5, prec, kernel)
+    for l, (cp, ri, vv) in enumerate(csc):
+        eng.set_layer_csc(nid, l, cp, ri, vv)
+    eng.build()
+    outs = []
+    for x, fmt in ((y0, cs.INPUT_U8), (bits, cs.INPUT_BITS), (y0.astype(np.float32), cs.INPUT_F32)):
+        eng.set_input(nid, x, fmt=fmt)
+        eng.run()
+        r = eng.result(nid)
+        outs.append((r, eng.final_values(nid, len(r["categories"]))))
+    eng.close()
+    for r, f in outs:
+        check_parity(r, ref, 4)
+        np.testing.assert_array_equal(f, outs[0][1])
