@@ -45,23 +45,19 @@ constexpr size_t kCcPairBudget = 96 * 1024;
 constexpr size_t kCcTileBudget = 200 * 1024;
 constexpr int kCcMaxTR = 128;
 
+// Entries per 16-byte group of the entry list.
 template <typename T>
-struct cc_traits;
-template <>
-struct cc_traits<float> {
-    static constexpr int V = 4, EPV = 2;  // rows per lane, entries per 16-byte group
-};
-template <>
-struct cc_traits<__half> {
-    static constexpr int V = 8, EPV = 4;
-};
-template <>
-struct cc_traits<__nv_bfloat16> {
-    static constexpr int V = 8, EPV = 4;
-};
+constexpr int cc_epv() {
+    return sizeof(T) == 4 ? 2 : 4;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+__device__ __forceinline__ uint2 lds64(uint32_t addr) {
+    uint2 v;
+    asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
+    return v;
+}
 __device__ __forceinline__ uint4 lds128(uint32_t addr) {
     uint4 v;
     asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
@@ -91,9 +87,22 @@ __device__ __forceinline__ void fma2(float &a0, float &a1, uint32_t ent, uint32_
         : "r"(ent), "r"(y));
 }
 
-// V FMAs of one entry on one 16-byte shared load (V rows of one input).
-template <typename T>
+// V = LB / elem FMAs of one entry on one LB-byte shared load (V rows of one
+// input).
+template <typename T, int LB>
 __device__ __forceinline__ void cc_entry(float *acc, uint32_t w, uint32_t addr) {
+    if constexpr (LB == 8) {
+        const uint2 y = lds64(addr);
+        if constexpr (sizeof(T) == 4) {
+            const float wf = __uint_as_float(w);
+            acc[0] = fmaf(wf, __uint_as_float(y.x), acc[0]);
+            acc[1] = fmaf(wf, __uint_as_float(y.y), acc[1]);
+        } else {
+            fma2(acc[0], acc[1], w, y.x, T());
+            fma2(acc[2], acc[3], w, y.y, T());
+        }
+        return;
+    }
     const uint4 y = lds128(addr);
     if constexpr (sizeof(T) == 4) {
         const float wf = __uint_as_float(w);
@@ -112,18 +121,19 @@ __device__ __forceinline__ void cc_entry(float *acc, uint32_t w, uint32_t addr) 
 // One block of four 16-byte groups of entries into the V accumulators: 16
 // entries of a 16-bit net ((column << 16) | weight bits, 4 per group) or 8 of
 // an FP32 net ({column, weight bits}, 2 per group); column = the input's
-// 16-byte column in the tile (input * G).
-template <typename T>
+// LB-byte column in the tile (input * G).
+template <typename T, int LB>
 __device__ __forceinline__ void cc_block(float *acc, const uint4 *q, uint32_t sbase) {
+    constexpr int SH = LB == 16 ? 4 : 3;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         if constexpr (sizeof(T) == 4) {
-            cc_entry<T>(acc, q[i].y, sbase + (q[i].x << 4));
-            cc_entry<T>(acc, q[i].w, sbase + (q[i].z << 4));
+            cc_entry<T, LB>(acc, q[i].y, sbase + (q[i].x << SH));
+            cc_entry<T, LB>(acc, q[i].w, sbase + (q[i].z << SH));
         } else {
             const uint32_t ent[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
 #pragma unroll
-            for (int e = 0; e < 4; ++e) cc_entry<T>(acc, ent[e], sbase + ((ent[e] >> 16) << 4));
+            for (int e = 0; e < 4; ++e) cc_entry<T, LB>(acc, ent[e], sbase + ((ent[e] >> 16) << SH));
         }
     }
 }
@@ -133,8 +143,15 @@ __device__ __forceinline__ void cc_load(uint4 *q, const uint4 *__restrict__ W, i
     for (int i = 0; i < 4; ++i) q[i] = __ldg(W + (int64_t)(b * 4 + i) * N + j);
 }
 
-__device__ __forceinline__ bool cc_net(const NetDev &nd, int prec) {
-    return nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 2 && nd.prec == prec && !nd.st->done;
+// Bytes of a feature column a lane owns: 16 when the tile's column has 16 or
+// more, else 8.
+__host__ __device__ __forceinline__ int cc_lane_bytes_of(int prec, int TR) {
+    return TR * (prec == COSPDNN_PREC_FP32 ? 4 : 2) >= 16 ? 16 : 8;
+}
+
+__device__ __forceinline__ bool cc_net(const NetDev &nd, int prec, int lb) {
+    return nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 2 && nd.prec == prec && !nd.st->done &&
+           cc_lane_bytes_of(nd.prec, nd.layout) == lb;
 }
 
 // Output slices per tile: the split (1, 2, 4, ... up to one CTA round of
@@ -143,7 +160,7 @@ __device__ __forceinline__ bool cc_net(const NetDev &nd, int prec) {
 __device__ __forceinline__ int cc_slices(const NetDev &nd, int grid, int warps) {
     const int TR = nd.layout, es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2;
     const int ntiles = (nd.st->R + TR - 1) / TR;
-    const int step = warps * (32 / (TR * es / 16));
+    const int step = warps * (32 / (TR * es / cc_lane_bytes_of(nd.prec, TR)));
     const int rounds = (nd.N + step - 1) / step;
     int best = 1;
     double best_cost = 1e30;
@@ -163,11 +180,11 @@ struct CcItem {
     int net, tile, slice, slices;
 };
 
-__device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int prec, int grid, int warps, int64_t u,
-                                          CcItem &it) {
+__device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int prec, int lb, int grid, int warps,
+                                          int64_t u, CcItem &it) {
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (!cc_net(nd, prec)) continue;
+        if (!cc_net(nd, prec, lb)) continue;
         const int S = cc_slices(nd, grid, warps);
         const int64_t cnt = (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * S;
         if (u < cnt) {
@@ -208,10 +225,10 @@ __device__ __forceinline__ void row_stats(float zm, float ez, float &emax, float
     emax = zm > -ez ? __fadd_ru(ez, store_error<T>(c)) : 0.0f;
 }
 
-// Bias, clamp, store of V accumulators as one 16-byte piece; max z per row.
-template <typename T>
+// Bias, clamp, store of V accumulators as one LB-byte piece; max z per row.
+template <typename T, int LB>
 __device__ __forceinline__ void cc_store(float *acc, float *zmax, float bias, T *dst) {
-    constexpr int V = cc_traits<T>::V;
+    constexpr int V = LB / (int)sizeof(T);
     __align__(16) T ov[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -220,15 +237,16 @@ __device__ __forceinline__ void cc_store(float *acc, float *zmax, float bias, T 
         ov[v] = act_traits<T>::from_f(clamp32(z));
         acc[v] = 0.0f;
     }
-    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(ov);
+    if constexpr (LB == 16) *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(ov);
+    else *reinterpret_cast<uint2 *>(dst) = *reinterpret_cast<const uint2 *>(ov);
 }
 
-template <typename T, int NT>
+template <typename T, int NT, int LB>
 __global__ void __launch_bounds__(NT, 512 / NT)
     k_layer_cc(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
     count_launch(launches);
-    constexpr int ES = (int)sizeof(T), V = cc_traits<T>::V, kWarps = NT / 32;
-    constexpr int EB = 4 * cc_traits<T>::EPV;  // entries per block
+    constexpr int ES = (int)sizeof(T), V = LB / ES, kWarps = NT / 32;
+    constexpr int EB = 4 * cc_epv<T>();  // entries per block
     extern __shared__ uint4 cc_smem[];
     __shared__ uint32_t s_zmax[kCcMaxTR];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -236,18 +254,18 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (!cc_net(nd, prec)) continue;
+        if (!cc_net(nd, prec, LB)) continue;
         total += (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * cc_slices(nd, grid, kWarps);
     }
     for (int64_t item = blockIdx.x; item < total; item += grid) {
         CcItem it;
-        cc_locate(nets, nnets, prec, grid, kWarps, item, it);
+        cc_locate(nets, nnets, prec, LB, grid, kWarps, item, it);
         const NetDev &nd = nets[it.net];
         const int N = nd.N, TR = nd.layout, l = nd.st->layer, R = nd.st->R, par = l & 1, ib = nd.st->in_buf;
         const LayerDev &lw = nd.layers[l];
         const T *in = (const T *)(l == 0 ? nd.y0 : nd.act[ib]);
         T *out = (T *)nd.act[ib ^ 1];
-        const int G = TR * ES / 16, lg = __ffs(G) - 1;  // lanes per output
+        const int G = TR * ES / LB, lg = __ffs(G) - 1;  // lanes per output
         const int opw = 32 >> lg;                        // outputs per warp and round
         const int c = lane & (G - 1), o = lane >> lg;
 
@@ -270,7 +288,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         if (threadIdx.x == 0 && item + grid < total) {
             // the next tile of this CTA into L2 while this one is computed
             CcItem nx;
-            if (cc_locate(nets, nnets, prec, grid, kWarps, item + grid, nx) &&
+            if (cc_locate(nets, nnets, prec, LB, grid, kWarps, item + grid, nx) &&
                 (nx.net != it.net || nx.tile != it.tile)) {
                 const NetDev &nn = nets[nx.net];
                 const T *nin = (const T *)(nn.st->layer == 0 ? nn.y0 : nn.act[nn.st->in_buf]);
@@ -290,7 +308,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         const int j_hi = min(N, ((it.slice + 1) * rounds / it.slices) * step);
         const int nb = lw.cc_k / EB;
         const uint4 *__restrict__ W = lw.cc_w;
-        const uint32_t sbase = smem_u32(cc_smem) + c * 16;
+        const uint32_t sbase = smem_u32(cc_smem) + c * LB;
         const float bias = nd.bias;
         const int j0 = j_lo + warp * opw + o;
         const int nout = j0 < j_hi ? (j_hi - j0 + step - 1) / step : 0;
@@ -312,7 +330,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         };
         auto finish_step = [&]() {
             if (++bc == nb) {
-                cc_store<T>(acc, zmax, bias, out + ((int64_t)it.tile * N + jc) * TR + c * V);
+                cc_store<T, LB>(acc, zmax, bias, out + ((int64_t)it.tile * N + jc) * TR + c * V);
                 bc = 0;
                 jc += step;
             }
@@ -321,15 +339,15 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         if (nsteps > 1) next_load(qb);
         for (int s = 0; s < nsteps; s += 3) {
             if (s + 2 < nsteps) next_load(qc);
-            cc_block<T>(acc, qa, sbase);
+            cc_block<T, LB>(acc, qa, sbase);
             finish_step();
             if (s + 1 >= nsteps) break;
             if (s + 3 < nsteps) next_load(qa);
-            cc_block<T>(acc, qb, sbase);
+            cc_block<T, LB>(acc, qb, sbase);
             finish_step();
             if (s + 2 >= nsteps) break;
             if (s + 4 < nsteps) next_load(qb);
-            cc_block<T>(acc, qc, sbase);
+            cc_block<T, LB>(acc, qc, sbase);
             finish_step();
         }
 
@@ -427,9 +445,11 @@ int colour_group(int P, const std::vector<int> &eu, const std::vector<int> &es, 
 int cc_tile_rows(int N, int prec) {
     const int es = prec == COSPDNN_PREC_FP32 ? 4 : 2;
     if (N > 65536) return 0;  // 16-bit input indices
-    for (size_t budget : {kCcPairBudget, kCcTileBudget})
-        for (int TR = kCcMaxTR; TR >= 2; TR >>= 1)
-            if (TR * es >= 16 && (size_t)N * TR * es <= budget) return TR;
+    // 16-byte lane columns (two CTAs per SM, then one), then 8-byte ones
+    for (int lb : {16, 8})
+        for (size_t budget : {kCcPairBudget, kCcTileBudget})
+            for (int TR = kCcMaxTR; TR >= 1; TR >>= 1)
+                if (TR * es >= lb && (size_t)N * TR * es <= budget) return TR;
     return 0;
 }
 
@@ -437,13 +457,18 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
                      const std::vector<float> &vals, int N, int prec, int TR, LayerDev &ld,
                      std::vector<void *> &owned) {
     const int es = prec == COSPDNN_PREC_FP32 ? 4 : 2;
-    const int colw = TR * es / 16;     // 16-byte columns per feature = lanes per output
-    const int B = colw >= 8 ? 1 : 8 / colw;  // outputs per quarter warp
-    const int P = B;                         // residues that must differ
+    // A lane owns an LB-byte piece of a feature column; shared loads are served
+    // 128 bytes at a time, i.e. by 128/LB lanes (a quarter warp for 16-byte,
+    // a half warp for 8-byte loads).
+    const int LB = cc_lane_bytes_of(prec, TR);
+    const int colw = TR * es / LB;                         // lanes per output
+    const int phase = 128 / LB;                            // lanes per wavefront
+    const int B = colw >= phase ? 1 : phase / colw;        // outputs per wavefront
+    const int P = B;                                       // residues that must differ
     CSP_CHECK(colw >= 1 && N % B == 0, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: bad tile");
     CSP_CHECK((size_t)N * colw <= 65536, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: tile too large");
     // groups of outputs whose entries must have distinct residues mod P at
-    // every step: the B outputs of a quarter warp
+    // every step: the B outputs of a wavefront
     std::vector<std::vector<int>> groups;
     for (int g0 = 0; g0 < N; g0 += B) {
         groups.emplace_back();
@@ -506,7 +531,7 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
                 }
                 const size_t g = (size_t)(t / epv), slot = (size_t)(t % epv);
                 uint32_t *dst = &packed[(g * N + j) * 4];
-                const uint32_t col = (uint32_t)idx * colw;  // first 16-byte column of the input
+                const uint32_t col = (uint32_t)idx * colw;  // first LB-byte column of the input
                 if (es == 4) {
                     dst[2 * slot] = col;
                     uint32_t wb;
@@ -529,14 +554,17 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
     return COSPDNN_OK;
 }
 
-int cc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms,
-                  size_t max_tile_bytes) {
+int cc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, int lane_bytes, unsigned long long *launches,
+                  int sms, size_t max_tile_bytes) {
     using F = void (*)(const NetDev *, int, int, unsigned long long *);
-    static const F fns[3][2] = {{k_layer_cc<float, 512>, k_layer_cc<float, 256>},
-                                {k_layer_cc<__half, 512>, k_layer_cc<__half, 256>},
-                                {k_layer_cc<__nv_bfloat16, 512>, k_layer_cc<__nv_bfloat16, 256>}};
+    static const F fns[3][2][2] = {
+        {{k_layer_cc<float, 512, 16>, k_layer_cc<float, 512, 8>}, {k_layer_cc<float, 256, 16>, k_layer_cc<float, 256, 8>}},
+        {{k_layer_cc<__half, 512, 16>, k_layer_cc<__half, 512, 8>},
+         {k_layer_cc<__half, 256, 16>, k_layer_cc<__half, 256, 8>}},
+        {{k_layer_cc<__nv_bfloat16, 512, 16>, k_layer_cc<__nv_bfloat16, 512, 8>},
+         {k_layer_cc<__nv_bfloat16, 256, 16>, k_layer_cc<__nv_bfloat16, 256, 8>}}};
     const bool pair = max_tile_bytes <= kCcPairBudget;
-    k.fn = (void *)fns[prec][pair ? 1 : 0];
+    k.fn = (void *)fns[prec][pair ? 1 : 0][lane_bytes == 16 ? 0 : 1];
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_tile_bytes));
     k.grid = dim3(pair ? 2 * sms : sms);
     k.block = dim3(pair ? 256 : 512);

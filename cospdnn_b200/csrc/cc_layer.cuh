@@ -17,9 +17,12 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
                      const std::vector<float> &vals, int N, int prec, int TR, LayerDev &ld,
                      std::vector<void *> &owned);
 // Launch description of the tile kernel for the CUDA-core row-tile nets of
-// precision `prec`; max_tile_bytes = largest N*TR*element size among them.
-int cc_layer_spec(KSpec &spec, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms,
-                  size_t max_tile_bytes);
+// precision `prec` whose lanes own `lane_bytes` (16 or 8) of a feature
+// column; max_tile_bytes = largest N*TR*element size among them.
+int cc_layer_spec(KSpec &spec, NetDev *nets, int nnets, int prec, int lane_bytes, unsigned long long *launches,
+                  int sms, size_t max_tile_bytes);
+// Lane bytes of a row-tile net of tile height TR.
+inline int cc_lane_bytes(int prec, int TR) { return TR * (prec == COSPDNN_PREC_FP32 ? 4 : 2) >= 16 ? 16 : 8; }
 // Bytes of one row tile.
 inline size_t cc_tile_bytes(int N, int prec, int TR) { return (size_t)N * TR * (prec == COSPDNN_PREC_FP32 ? 4 : 2); }
 

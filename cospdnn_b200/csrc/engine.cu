@@ -203,6 +203,7 @@ struct cospdnn_engine {
     int max_n = 0, max_layers = 0;
     double *scratch = nullptr;
     int replay_ctas = 0;
+    int compact_ctas = 0;  // compaction chunks of all nets at full size
     unsigned long long *launches = nullptr;
     unsigned int *finished = nullptr;
     int *loop_guard = nullptr;
@@ -283,8 +284,8 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
 // Precisions of the nets on each layer kernel.
 struct KernelSets {
     std::vector<int> plain, tc;
-    // row-tile kernel: precision -> largest row tile of those nets
-    std::vector<std::pair<int, size_t>> cc;
+    // row-tile kernel: (precision, lane bytes) -> largest row tile of those nets
+    std::vector<std::pair<std::pair<int, int>, size_t>> cc;
 };
 
 int make_specs(cospdnn_engine *e, const KernelSets &ks) {
@@ -313,7 +314,7 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
     }
     for (const auto &cc : ks.cc) {
         KSpec k;
-        int rc = cc_layer_spec(k, nets, nn, cc.first, launches, sms, cc.second);
+        int rc = cc_layer_spec(k, nets, nn, cc.first.first, cc.first.second, launches, sms, cc.second);
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
@@ -343,7 +344,7 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
     for (int use_cond = 0; use_cond < 2; ++use_cond) {
         KSpec &k4 = use_cond ? e->k4_graph : e->k4_eager;
         k4.fn = (void *)k_compact;
-        k4.grid = dim3(nn);
+        k4.grid = dim3(e->compact_ctas);
         k4.block = dim3(kCompactThreads);
         k4.arg(nets).arg(nn).arg(e->finished).arg(e->loop).arg(use_cond).arg(guard)
             .arg(e->max_layers + 2).arg((const int *)e->abort_flag).arg(launches);
@@ -536,7 +537,7 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         // kernel) or row-major (CUDA-core gather kernel, rows too wide for a tile)
         n.dev.layout = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? 1 : cc_tile_rows(n.d.neuron, n.d.precision);
         if (n.dev.layout >= 2) {
-            const int key = n.d.precision;
+            const std::pair<int, int> key(n.d.precision, cc_lane_bytes(n.d.precision, n.dev.layout));
             const size_t tb = cc_tile_bytes(n.d.neuron, n.d.precision, n.dev.layout);
             auto it = std::find_if(ks.cc.begin(), ks.cc.end(), [&](const auto &x) { return x.first == key; });
             if (it == ks.cc.end()) ks.cc.push_back({key, tb});
@@ -583,6 +584,11 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         d.stat = dalloc<uint32_t>((size_t)3 * R, e->owned);
         d.cls = dalloc<int8_t>(R, e->owned);
         d.ulist = dalloc<int32_t>(R, e->owned);
+        const int nchunks = (R + kCompactChunk - 1) / kCompactChunk;
+        d.ccount = dalloc<int32_t>(nchunks, e->owned);
+        CSP_CHECK(d.ccount, COSPDNN_ERR_NOMEM, "build: device allocation failed");
+        CSP_CUDA(cudaMemset(d.ccount, 0, sizeof(int32_t) * nchunks));
+        e->compact_ctas += nchunks;
         d.alive_count = dalloc<long long>(d.L, e->owned);
         d.recheck_count = dalloc<long long>(d.L, e->owned);
         d.st = dalloc<NetState>(1, e->owned);

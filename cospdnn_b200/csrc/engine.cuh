@@ -98,12 +98,16 @@ struct NetDev {
     uint32_t *stat;          // [rows][3]: ordered max z, e_out bits, m_out bits
     int8_t *cls;             // [rows] 0 prune, 1 keep, 2 uncertain
     int32_t *ulist;          // [rows] uncertain positions
+    int32_t *ccount;         // [rows / kCompactChunk, rounded up] kept rows per chunk of this layer
     long long *alive_count;  // [L] rows kept after layer l
     long long *recheck_count;// [L] rows re-decided in FP64 at layer l
     NetState *st;
 };
 
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
+
+// Rows per compaction chunk (one CTA of k_compact; a multiple of 32).
+constexpr int kCompactChunk = 1024;
 
 // Element index of (row, feature) in an activation buffer of width N.
 // layout 0, row-major: row*N + f.

@@ -42,6 +42,7 @@ __global__ void k_init_run(const NetDev *__restrict__ nets, int nnets, unsigned 
             nd.alive_count[l] = 0;
             nd.recheck_count[l] = 0;
         }
+        for (int64_t c = tid; c < (nd.rows + kCompactChunk - 1) / kCompactChunk; c += nth) nd.ccount[c] = 0;
         for (int64_t p = tid; p < nd.rows; p += nth) {
             nd.orig[0][p] = (int32_t)p;
             nd.err[0][p] = nd.err0[p];
@@ -148,26 +149,34 @@ __global__ void __launch_bounds__(kPlainThreads)
 }
 
 // ---- K2: keep / prune / uncertain per row ---------------------------------
+// A warp takes 32 consecutive rows (all in one compaction chunk) and adds its
+// sure keeps to the chunk's count; k_replay adds the re-decided ones.
 __global__ void k_classify(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
     count_launch(launches);
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (nd.st->done) continue;
         const int l = nd.st->layer, R = nd.st->R, par = l & 1;
         const LayerDev &lw = nd.layers[l];
         const double steps = fast_steps(nd, lw);
-        for (int64_t p = tid; p < R; p += nth) {
-            const float zm = ord2f(nd.stat[3 * p]);
-            const float ez = z_error_bound(nd.err[par][p], nd.mx[par][p], lw.S, lw.dW, nd.bias, steps);
-            const double lo = (double)zm - (double)ez, hi = (double)zm + (double)ez;
-            int8_t c;
-            if (lo > (double)nd.tau) c = CLS_KEEP;
-            else if (hi <= (double)nd.tau) c = CLS_PRUNE;
-            else c = CLS_UNCERTAIN;
-            nd.cls[p] = c;
-            if (c == CLS_UNCERTAIN) nd.ulist[atomicAdd(&nd.st->nunc, 1)] = (int32_t)p;
+        for (int64_t base = warp * 32; base < R; base += nwarps * 32) {
+            const int64_t p = base + lane;
+            int8_t c = CLS_PRUNE;
+            if (p < R) {
+                const float zm = ord2f(nd.stat[3 * p]);
+                const float ez = z_error_bound(nd.err[par][p], nd.mx[par][p], lw.S, lw.dW, nd.bias, steps);
+                const double lo = (double)zm - (double)ez, hi = (double)zm + (double)ez;
+                if (lo > (double)nd.tau) c = CLS_KEEP;
+                else if (hi <= (double)nd.tau) c = CLS_PRUNE;
+                else c = CLS_UNCERTAIN;
+                nd.cls[p] = c;
+                if (c == CLS_UNCERTAIN) nd.ulist[atomicAdd(&nd.st->nunc, 1)] = (int32_t)p;
+            }
+            const unsigned keep = __ballot_sync(0xffffffffu, c == CLS_KEEP);
+            if (lane == 0 && keep) atomicAdd(&nd.ccount[base / kCompactChunk], __popc(keep));
         }
     }
 }
@@ -179,7 +188,7 @@ __global__ void k_classify(const NetDev *__restrict__ nets, int nnets, unsigned 
 // keep/prune exactly, and for kept rows overwrite the fast output with the
 // FP64 values rounded to the compute type.  The row is held in shared memory
 // when two copies fit (kReplaySmemN doubles each), else in global scratch.
-constexpr int kReplayThreads = 512;
+constexpr int kReplayThreads = 1024;
 constexpr int kReplaySmemN = 8192;
 
 __device__ __forceinline__ float block_max(float v, float *red) {
@@ -216,16 +225,16 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
             const int32_t *ip = lw.ell_idx + j;
             const float *wp = lw.ell_val + j;
             int k = 0;
-            for (; k + 8 <= lw.K; k += 8) {
-                int32_t ii[8];
-                float ww[8];
+            for (; k + 32 <= lw.K; k += 32) {
+                int32_t ii[32];
+                float ww[32];
 #pragma unroll
-                for (int t = 0; t < 8; ++t) {
+                for (int t = 0; t < 32; ++t) {
                     ii[t] = __ldg(ip + (int64_t)(k + t) * N);
                     ww[t] = __ldg(wp + (int64_t)(k + t) * N);
                 }
 #pragma unroll
-                for (int t = 0; t < 8; ++t) {
+                for (int t = 0; t < 32; ++t) {
                     const double yi = y[ii[t]];
                     if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn((double)ww[t], yi));
                 }
@@ -259,6 +268,7 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
     if (threadIdx.x == 0) {
         nd.cls[p] = keep ? CLS_KEEP : CLS_PRUNE;
         if (keep) {
+            atomicAdd(&nd.ccount[p / kCompactChunk], 1);
             nd.stat[3 * p + 1] = __float_as_uint(emax);
             nd.stat[3 * p + 2] = __float_as_uint(ymax);
         }
@@ -300,108 +310,132 @@ __global__ void __launch_bounds__(kReplayThreads)
 }
 
 // ---- K4: stable compaction + state advance + loop condition ---------------
-constexpr int kCompactThreads = 1024;
+// One CTA per chunk of kCompactChunk rows (grid = chunks of all nets at full
+// size; chunks past a net's current rows are idle).  A chunk's first output
+// position is the sum of the keep counts of the chunks before it.  The last
+// CTA to finish advances every net's state and decides whether the graph
+// loop runs again.
+constexpr int kCompactThreads = kCompactChunk;
 
 __global__ void __launch_bounds__(kCompactThreads)
     k_compact(const NetDev *__restrict__ nets, int nnets, unsigned int *finished_ctas,
               cudaGraphConditionalHandle loop, int use_cond, int *loop_guard, int max_iters,
               const int *abort_flag, unsigned long long *launches) {
     count_launch(launches);
-    __shared__ int warp_tot[kCompactThreads / 32];
-    __shared__ int carry, s_done, s_layer, s_R;
-    const int n = blockIdx.x;
-    const NetDev &nd = nets[n];
+    __shared__ int red[kCompactThreads / 32];
+    __shared__ int s_base;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (threadIdx.x == 0) {
-        s_done = nd.st->done;
-        s_layer = nd.st->layer;
-        s_R = nd.st->R;
-        carry = 0;
+    // locate this CTA's chunk
+    int64_t u = blockIdx.x;
+    int n = 0;
+    for (; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        const int64_t cnt = nd.st->done ? 0 : (nd.st->R + kCompactChunk - 1) / kCompactChunk;
+        if (u < cnt) break;
+        u -= cnt;
     }
-    __syncthreads();
-    if (!s_done) {
-        const int l = s_layer, R = s_R, par = l & 1;
-        constexpr int kRun = 8;  // consecutive rows per thread and pass (stable order)
-        for (int base = 0; base < R; base += kCompactThreads * kRun) {
-            const int p0 = base + threadIdx.x * kRun;
-            uint32_t keep = 0;
+    if (n < nnets) {
+        const NetDev &nd = nets[n];
+        const int l = nd.st->layer, R = nd.st->R, par = l & 1, b = (int)u;
+        // kept rows of the chunks before this one
+        int v = 0;
+        for (int t = threadIdx.x; t < b; t += kCompactThreads) v += nd.ccount[t];
 #pragma unroll
-            for (int i = 0; i < kRun; ++i)
-                if (p0 + i < R && nd.cls[p0 + i] == CLS_KEEP) keep |= 1u << i;
-            int v = __popc(keep);
-            // inclusive scan of the per-thread counts over the warp, then the warps
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[wid] = v;
+        __syncthreads();
+        if (wid == 0) {
+            int w = red[lane];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+            if (lane == 0) s_base = w;
+        }
+        __syncthreads();
+        // stable scan of this chunk's keeps
+        const int p = b * kCompactChunk + threadIdx.x;
+        const int keep = (p < R && nd.cls[p] == CLS_KEEP) ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) red[wid] = __popc(m);
+        __syncthreads();
+        if (wid == 0) {
+            int w = red[lane];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += t;
+                const int t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += t;
             }
-            if (lane == 31) warp_tot[wid] = v;
-            __syncthreads();
-            if (wid == 0) {
-                int w = warp_tot[lane];
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, w, o);
-                    if (lane >= o) w += t;
-                }
-                warp_tot[lane] = w;
-            }
-            __syncthreads();
-            int q = carry + (wid ? warp_tot[wid - 1] : 0) + v - __popc(keep);
-#pragma unroll
-            for (int i = 0; i < kRun; ++i) {
-                const int p = p0 + i;
-                if ((keep >> i) & 1u) {
-                    nd.cmap[q] = p;
-                    nd.orig[par ^ 1][q] = nd.orig[par][p];
-                    nd.err[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 1]);
-                    nd.mx[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 2]);
-                    ++q;
-                }
-                if (p < R) {
-                    nd.stat[3 * p] = 0u;
-                    nd.stat[3 * p + 1] = 0u;
-                    nd.stat[3 * p + 2] = 0u;
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) carry += warp_tot[kCompactThreads / 32 - 1];
-            __syncthreads();
+            red[lane] = w;
         }
+        __syncthreads();
+        if (keep) {
+            const int q = s_base + (wid ? red[wid - 1] : 0) + __popc(m & ((1u << lane) - 1u));
+            nd.cmap[q] = p;
+            nd.orig[par ^ 1][q] = nd.orig[par][p];
+            nd.err[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 1]);
+            nd.mx[par ^ 1][q] = __uint_as_float(nd.stat[3 * p + 2]);
+        }
+        if (p < R) {
+            nd.stat[3 * p] = 0u;
+            nd.stat[3 * p + 1] = 0u;
+            nd.stat[3 * p + 2] = 0u;
+        }
+    }
+    // the last CTA to finish advances the states and sets the loop condition
+    __syncthreads();
+    __shared__ int s_last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(finished_ctas, 1u) + 1u == gridDim.x;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int i = 0; i < nnets; ++i) {
+        const NetDev &nd = nets[i];
+        if (*(volatile int *)&nd.st->done) {
+            if (threadIdx.x == 0) nd.st->copy_R = 0;
+            continue;
+        }
+        const int l = nd.st->layer, R = nd.st->R, nch = (R + kCompactChunk - 1) / kCompactChunk;
+        int v = 0;
+        for (int t = threadIdx.x; t < nch; t += kCompactThreads) {
+            v += *(volatile int32_t *)&nd.ccount[t];
+            nd.ccount[t] = 0;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        __syncthreads();
+        if (lane == 0) red[wid] = v;
+        __syncthreads();
         if (threadIdx.x == 0) {
-            nd.alive_count[l] = carry;
+            int kept = 0;
+            for (int w = 0; w < kCompactThreads / 32; ++w) kept += red[w];
+            nd.alive_count[l] = kept;
             nd.recheck_count[l] = nd.st->nunc;
             nd.st->nunc = 0;
-            nd.st->R = carry;
+            nd.st->R = kept;
             nd.st->layer = l + 1;
-            nd.st->done = (carry == 0 || l + 1 >= nd.L);
-            if (carry == R) {
+            nd.st->done = (kept == 0 || l + 1 >= nd.L);
+            if (kept == R) {
                 // nothing pruned: the output buffer is the next input as it is
                 nd.st->in_buf ^= 1;
                 nd.st->copy_R = 0;
             } else {
-                nd.st->copy_R = carry;  // k_copy_rows moves the kept rows
+                nd.st->copy_R = kept;  // k_copy_rows moves the kept rows
             }
         }
-    } else if (threadIdx.x == 0) {
-        nd.st->copy_R = 0;
     }
-    // the last CTA to finish decides whether the graph loop runs again
     if (threadIdx.x == 0) {
+        *finished_ctas = 0u;
         __threadfence();
-        const unsigned done_ctas = atomicAdd(finished_ctas, 1u) + 1u;
-        if (done_ctas == (unsigned)gridDim.x) {
-            *finished_ctas = 0u;
-            __threadfence();
-            int live = 0;
-            for (int i = 0; i < nnets; ++i) live |= !(*(volatile int *)&nets[i].st->done);
-            const int it = ++*loop_guard;
-            if (it > max_iters || *(volatile const int *)abort_flag) {
-                for (int i = 0; i < nnets; ++i) nets[i].st->err = COSPDNN_ERR_DEVICE;
-                live = 0;
-            }
-            if (use_cond) cudaGraphSetConditional(loop, live ? 1u : 0u);
+        int live = 0;
+        for (int i = 0; i < nnets; ++i) live |= !(*(volatile int *)&nets[i].st->done);
+        const int it = ++*loop_guard;
+        if (it > max_iters || *(volatile const int *)abort_flag) {
+            for (int i = 0; i < nnets; ++i) nets[i].st->err = COSPDNN_ERR_DEVICE;
+            live = 0;
         }
+        if (use_cond) cudaGraphSetConditional(loop, live ? 1u : 0u);
     }
 }
 
@@ -409,38 +443,127 @@ __global__ void __launch_bounds__(kCompactThreads)
 // Row q of act[in_buf] <- row cmap[q] of act[in_buf ^ 1].
 // Row-major and MMA-tile nets: 16-byte pieces (row-major: consecutive; MMA
 // tiles: the two 8-feature halves of each block).  Row-tile nets: one CTA per
-// destination tile, which is written contiguously (feature-major, TR values
-// per feature; rows past the kept count are zero).
+// destination tile; the source tiles its rows come from (a contiguous range,
+// the map being increasing) are staged in shared memory a feature chunk at a
+// time with 16-byte loads, and the destination tile is written contiguously
+// (rows past the kept count are zero).
+constexpr int kCopyThreads = 256;
+constexpr int kCopyStageBytes = 40 * 1024;
+
+// Copies `pieces` U-sized pieces from global to shared memory, 8 in flight
+// per thread.
+template <typename U>
+__device__ __forceinline__ void stage_pieces(U *to, const U *__restrict__ from, int pieces) {
+    int k = threadIdx.x;
+    for (; k + 7 * kCopyThreads < pieces; k += 8 * kCopyThreads) {
+        U v[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[t] = __ldg(from + k + t * kCopyThreads);
+#pragma unroll
+        for (int t = 0; t < 8; ++t) to[k + t * kCopyThreads] = v[t];
+    }
+    for (; k < pieces; k += kCopyThreads) to[k] = __ldg(from + k);
+}
+
+// One destination row tile; U = the piece type of one feature column when a
+// column is 8 or 16 bytes (columns of 32 bytes and more use 16-byte pieces).
+constexpr int kCopyFeatures = 64;  // fewest features per work item of a row-tile copy
+
+// Feature chunks per destination tile of a row-tile copy: enough items for
+// about two per CTA of the grid, chunks of at least kCopyFeatures.
+__device__ __forceinline__ int copy_chunks(const NetDev &nd, int grid) {
+    const int tiles = (nd.st->copy_R + nd.layout - 1) / nd.layout;
+    const int most = (nd.N + kCopyFeatures - 1) / kCopyFeatures;
+    if (tiles == 0) return 1;
+    return max(1, min(most, (2 * grid + tiles - 1) / tiles));
+}
+
 template <typename E>
-__device__ __forceinline__ void copy_tile(const NetDev &nd, int tq, int64_t *s_src) {
+__device__ __forceinline__ void copy_tile(const NetDev &nd, int tq, int fbeg, int fend, uint4 *stage) {
+    // s_src[k]: the k-th distinct source tile of this tile's rows (the map is
+    // increasing, so they come in order); row r reads slot s_tile[r], row
+    // s_off[r] of it (s_tile = -1: past the kept rows)
+    __shared__ int s_tile[128], s_off[128], s_src[128], s_raw[128];
     const int N = nd.N, TR = nd.layout, ib = nd.st->in_buf, R = nd.st->copy_R;
     const E *src = (const E *)nd.act[ib ^ 1];
     E *dst = (E *)nd.act[ib] + (int64_t)tq * N * TR;
-    __syncthreads();
+    __syncthreads();  // the previous tile is done with the shared arrays
     for (int r = threadIdx.x; r < TR; r += blockDim.x) {
         const int q = tq * TR + r;
-        s_src[r] = q < R ? act_index(TR, N, nd.cmap[q], 0) : -1;
+        const int p = q < R ? nd.cmap[q] : -1;
+        s_raw[r] = p < 0 ? -1 : p / TR;
+        s_off[r] = p < 0 ? 0 : p % TR;
     }
     __syncthreads();
-    const int lg = __ffs(TR) - 1;
-    const int total = N * TR;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-        const int r = i & (TR - 1), f = i >> lg;
-        const int64_t o = s_src[r];
-        dst[i] = o >= 0 ? src[o + (int64_t)f * TR] : E(0);
+    for (int r = threadIdx.x; r < TR; r += blockDim.x) {
+        const int t = s_raw[r];
+        int rank = -1;
+        if (t >= 0) {
+            rank = 0;
+            for (int k = 1; k <= r; ++k) rank += s_raw[k] != s_raw[k - 1];
+            if (r == 0 || s_raw[r - 1] != t) s_src[rank] = t;
+        }
+        s_tile[r] = rank;
+    }
+    __syncthreads();
+    int nsrc = 0;
+    for (int r = 0; r < TR; ++r) nsrc = max(nsrc, s_tile[r] + 1);
+    const int colb = TR * (int)sizeof(E);  // bytes of a feature column: 8 or a multiple of 16
+    const int fc_max = kCopyStageBytes / (nsrc * colb);
+    const E *sst = (const E *)stage;
+    if (fc_max == 0) {
+        // one feature column of every source tile does not fit: gather directly
+        for (int i = fbeg * TR + threadIdx.x; i < fend * TR; i += blockDim.x) {
+            const int f = i / TR, r = i - f * TR, t = s_tile[r];
+            dst[i] = t >= 0 ? src[((int64_t)s_src[t] * N + f) * TR + s_off[r]] : E(0);
+        }
+        return;
+    }
+    for (int f0 = fbeg; f0 < fend; f0 += fc_max) {
+        const int fc = min(fc_max, fend - f0);
+        for (int sidx = 0; sidx < nsrc; ++sidx) {
+            const E *from = src + ((int64_t)s_src[sidx] * N + f0) * TR;
+            E *to = (E *)stage + (int64_t)sidx * fc_max * TR;
+            if (colb == 8)
+                stage_pieces(reinterpret_cast<uint2 *>(to), reinterpret_cast<const uint2 *>(from), fc);
+            else
+                stage_pieces(reinterpret_cast<uint4 *>(to), reinterpret_cast<const uint4 *>(from), fc * colb / 16);
+        }
+        __syncthreads();
+        {
+            // destination columns in 16-byte pieces (one 8-byte piece for an
+            // 8-byte column): kV consecutive rows of one feature per store
+            constexpr int kV = 16 / (int)sizeof(E);
+            const int pcs = colb >= 16 ? colb / 16 : 1;  // pieces per feature
+            for (int u = threadIdx.x; u < fc * pcs; u += kCopyThreads) {
+                const int fl = u / pcs, r0 = (u - fl * pcs) * kV;
+                __align__(16) E col[kV];
+#pragma unroll
+                for (int v = 0; v < kV; ++v) {
+                    const int r = r0 + v;
+                    const int t = r < TR ? s_tile[r] : -1;
+                    col[v] = t >= 0 ? sst[(int64_t)t * fc_max * TR + fl * TR + s_off[r]] : E(0);
+                }
+                E *d = dst + (int64_t)(f0 + fl) * TR + r0;
+                if (colb >= 16) *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(col);
+                else *reinterpret_cast<uint2 *>(d) = *reinterpret_cast<const uint2 *>(col);
+            }
+        }
+        __syncthreads();
     }
 }
 
-__global__ void k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
+__global__ void __launch_bounds__(kCopyThreads)
+    k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
     count_launch(launches);
-    __shared__ int64_t s_src[128];
+    __shared__ uint4 stage[kCopyStageBytes / 16];
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
     int64_t total = 0, tiles = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (nd.layout >= 2) {
-            tiles += (nd.st->copy_R + nd.layout - 1) / nd.layout;
+            tiles += (int64_t)((nd.st->copy_R + nd.layout - 1) / nd.layout) * copy_chunks(nd, gridDim.x);
             continue;
         }
         const int es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2;
@@ -467,18 +590,23 @@ __global__ void k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned
         const uint4 v = *reinterpret_cast<const uint4 *>(src + act_index(nd.layout, N, p, f) * es);
         *reinterpret_cast<uint4 *>(dst + act_index(nd.layout, N, q, f) * es) = v;
     }
+    // row-tile nets: items of (destination tile, feature chunk)
     for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         int64_t u = t;
-        int n = 0;
+        int n = 0, nfc = 1;
         for (; n < nnets; ++n) {
             const NetDev &nd = nets[n];
             if (nd.layout < 2) continue;
-            const int64_t cnt = (nd.st->copy_R + nd.layout - 1) / nd.layout;
+            nfc = copy_chunks(nd, gridDim.x);
+            const int64_t cnt = (int64_t)((nd.st->copy_R + nd.layout - 1) / nd.layout) * nfc;
             if (u < cnt) break;
             u -= cnt;
         }
-        if (nets[n].prec == COSPDNN_PREC_FP32) copy_tile<uint32_t>(nets[n], (int)u, s_src);
-        else copy_tile<uint16_t>(nets[n], (int)u, s_src);
+        const int per = ((nets[n].N + nfc - 1) / nfc + 7) / 8 * 8;  // features per chunk
+        const int tq = (int)(u / nfc), fb = min(nets[n].N, (int)(u % nfc) * per);
+        const int fe = min(nets[n].N, fb + per);
+        if (nets[n].prec == COSPDNN_PREC_FP32) copy_tile<uint32_t>(nets[n], tq, fb, fe, stage);
+        else copy_tile<uint16_t>(nets[n], tq, fb, fe, stage);
     }
 }
 

@@ -151,9 +151,10 @@ def test_engine_tcgen05_layer_values_match_cuda_core(cs):
 
 # Row-tile heights of the CUDA-core tile kernel (tile = N x TR values in at
 # most 200 KB of shared memory): each case exercises a different number of
-# lanes per output (G) and outputs per quarter warp (P = 8/G).
-@pytest.mark.parametrize("n,prec", [(512, 1), (1000, 1), (2048, 2), (3000, 1), (8192, 1),
-                                    (512, 0), (1000, 0), (4096, 0)])
+# lanes per output (G) and outputs per shared-memory wavefront (P); 16384
+# features take 8-byte lane pieces (P = 16).
+@pytest.mark.parametrize("n,prec", [(512, 1), (1000, 1), (2048, 2), (3000, 1), (8192, 1), (16384, 2),
+                                    (512, 0), (1000, 0), (4096, 0), (16384, 0)])
 def test_engine_cc_tile_shapes(cs, n, prec):
     from netgen import make_random_net
     csc, y0, b = make_random_net(n, 5, 333, seed=23)
@@ -179,9 +180,9 @@ def test_engine_cc_random_weights_sustained(cs, n, prec):
 
 
 def test_engine_row_major_gather_kernel_wide_fp32(cs):
-    """FP32 rows of 16384 features do not fit a 16-byte row tile in shared
-    memory: the net runs on the row-major gather kernel."""
-    csc, y0, b = make_net(16384, 4, 200, seed=31, dlo=0.2, dhi=0.4)
+    """FP32 rows of 32768 features do not fit a row tile in shared memory:
+    the net runs on the row-major gather kernel."""
+    csc, y0, b = make_net(32768, 4, 200, seed=31, dlo=0.2, dhi=0.4)
     ref = oracle_run(csc, y0, b)
     res = run_engine(cs, [(csc, y0, b)], 0, 1)[0]
     check_parity(res, ref, 4)
@@ -211,7 +212,8 @@ def test_engine_mixed_kernels_one_graph(cs):
         check_parity(r, f, len(n[0]))
 
 
-@pytest.mark.parametrize("n,prec,kernel", [(1000, 1, 1), (4096, 1, 1), (1024, 0, 1), (4096, 2, 2), (16384, 0, 1)])
+@pytest.mark.parametrize("n,prec,kernel", [(1000, 1, 1), (4096, 1, 1), (1024, 0, 1), (4096, 2, 2), (16384, 1, 1),
+                                           (32768, 0, 1)])
 def test_engine_input_formats_agree(cs, n, prec, kernel):
     """Bytes, packed bits (little-endian within a byte) and float32 inputs of
     the same binary rows give identical results (row tiles, MMA tiles and
