@@ -49,7 +49,26 @@ def build(force=False, verbose=False):
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
         subprocess.run([nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs], check=True)
+    build_cli(force)
     return LIB
+
+
+CLI = os.path.join(HERE, "cli")
+CLI_PROGRAMS = ["cospdnn", "cospdnn_double"]
+
+
+def build_cli(force=False):
+    """The reference's command lines (cli/cospdnn.out, cli/cospdnn_double.out):
+    host C++ over the C ABI, linked against the in-tree library."""
+    cxx = shutil.which("g++") or "g++"
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    deps = [os.path.join(CLI, "reference_io.h"), os.path.join(inc, "cospdnn_b200.h"), LIB]
+    for prog in CLI_PROGRAMS:
+        src = os.path.join(CLI, prog + ".cpp")
+        out = os.path.join(CLI, prog + ".out")
+        if force or _stale(out, [src] + deps):
+            subprocess.run([cxx, "-O2", "-std=c++17", "-Wall", "-I", inc, src, "-o", out, "-L", HERE,
+                            "-lcospdnn_b200", "-Wl,-rpath,$ORIGIN/..", "-pthread"], check=True)
 
 
 if __name__ == "__main__":

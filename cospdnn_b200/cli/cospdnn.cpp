@@ -1,0 +1,85 @@
+// cospdnn.out: one network, the reference's command line
+// (src/cospdnn.cpp:80-189):
+//     cospdnn.out neuron batch layer gpu_num gpu_id dataset_dir
+// Reads the dataset files (reference_io.h), runs every layer on the engine
+// (one graph launch per GPU) and prints the reference's lines
+// "layer l, feature = n" (rows alive after layer l) and
+// "Kernel Exec Time = X ms".  With gpu_num > 1 the batch is split into
+// contiguous row ranges, one engine and host thread per GPU, and the counts
+// are summed.  COSPDNN_PRECISION / COSPDNN_KERNEL select precision and kernel.
+#include <algorithm>
+#include <thread>
+
+#include "reference_io.h"
+
+using namespace cospdnn_cli;
+
+int main(int argc, char *argv[]) {
+    if (argc != 7) {
+        std::cout << "Usage: exe neuron batch layer gpu_num gpu_id dataset_dir" << std::endl;
+        return 0;
+    }
+    const int neuron = std::atoi(argv[1]), batch = std::atoi(argv[2]), layers = std::atoi(argv[3]);
+    int gpu_num = std::atoi(argv[4]);
+    const int dev = std::atoi(argv[5]);
+    const std::string dir(argv[6]);
+    if (neuron <= 0 || batch <= 0 || layers <= 0 || gpu_num <= 0) die("bad arguments");
+    std::cout << "[BEGIN]..." << std::endl;
+    std::cout << "[Batch] :" << batch << std::endl;
+    std::cout << "[Neuron] :" << neuron << std::endl;
+    std::cout << "[Layer] :" << layers << std::endl;
+    const Network net = load_network(neuron, batch, layers, dir);
+    const int prec = env_precision(), kern = env_kernel();
+
+    std::vector<int> devices;
+    if (gpu_num == 1) {
+        devices.push_back(dev);
+    } else {
+        const int avail = cospdnn_device_count();
+        if (gpu_num > avail) {
+            std::cout << "Exceeding Maximum GPU Number! Automatically Change to Max GPU Number " << avail << std::endl;
+            gpu_num = avail;
+        }
+        for (int g = 0; g < gpu_num; ++g) devices.push_back(g);
+    }
+    const int ng = (int)devices.size();
+    std::vector<std::vector<int64_t>> alive(ng, std::vector<int64_t>(layers, 0));
+    std::vector<int64_t> count(ng, 0);
+    std::vector<float> ms(ng, 0.0f);
+    // each worker exits the process with the reference's style of message on
+    // any error (as Safe_Call does in the reference)
+    auto work = [&](int g) {
+        const int r0 = (int)((int64_t)batch * g / ng), r1 = (int)((int64_t)batch * (g + 1) / ng);
+        cospdnn_engine *e = nullptr;
+        check(cospdnn_engine_create(&e, devices[g]), "engine_create");
+        const int id = add_network(e, net, r0, r1, prec, kern);
+        check(cospdnn_engine_build(e), "build");
+        set_rows(e, id, net, r0, r1);
+        check(cospdnn_engine_run_timed(e, nullptr, &ms[g]), "run");
+        check(cospdnn_engine_result(e, id, nullptr, &count[g], alive[g].data(), nullptr, nullptr), "result");
+        cospdnn_engine_destroy(e);
+    };
+    if (ng == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (int g = 0; g < ng; ++g) th.emplace_back(work, g);
+        for (auto &t : th) t.join();
+    }
+    int64_t total = 0;
+    for (int g = 0; g < ng; ++g) total += count[g];
+    for (int l = 0; l < layers; ++l) {
+        int64_t f = 0;
+        for (int g = 0; g < ng; ++g) f += alive[g][l];
+        std::cout << "layer " << l << ", feature = " << f << std::endl;
+    }
+    float tmax = 0.0f;
+    for (int g = 0; g < ng; ++g) {
+        if (ng > 1) std::cout << "GPU[" << devices[g] << "] Kernel Exec Time = " << ms[g] << "ms" << std::endl;
+        tmax = std::max(tmax, ms[g]);
+    }
+    std::cout << "[Categories] :" << total << std::endl;
+    std::cout << "Kernel Exec Time = " << tmax << "ms" << std::endl;
+    std::cout << "[END]..." << std::endl;
+    return 0;
+}

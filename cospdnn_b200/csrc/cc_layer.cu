@@ -210,30 +210,33 @@ __device__ __forceinline__ float store_error(float c) {
     else return __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
 }
 
-// Row statistics from the row's max pre-activation zm and its error bound ez:
+// Row statistics from the row's max pre-activation zm, its min |z - 16|
+// over the outputs (zd) and its error bound ez:
 //   max output  = the stored value of clamp(zm) (rounding is monotone, so
 //                 this is the max of the stored outputs);
 //   output error: outputs with z <= -ez are 0 in both recurrences and those
-//                 with z >= 32 + ez are 32 in both; any other output is
-//                 within ez of the exact clamp plus its storage rounding, and
-//                 is at most clamp(zm): bound ez + store_error(clamp(zm)) when
-//                 zm > -ez, else 0.
+//                 with z >= 32 + ez are 32 in both; the others, those with
+//                 |z - 16| < 16 + ez (there are some iff zd < 16 + ez), are
+//                 within ez of the exact clamp plus their storage rounding,
+//                 at most clamp(zm): bound ez + store_error(clamp(zm)), else 0.
 template <typename T>
-__device__ __forceinline__ void row_stats(float zm, float ez, float &emax, float &ymax) {
+__device__ __forceinline__ void row_stats(float zm, float zd, float ez, float &emax, float &ymax) {
     const float c = clamp32(zm);
     ymax = act_traits<T>::to_f(act_traits<T>::from_f(c));
-    emax = zm > -ez ? __fadd_ru(ez, store_error<T>(c)) : 0.0f;
+    emax = zd < 16.0f + ez ? __fadd_ru(ez, store_error<T>(c)) : 0.0f;
 }
 
-// Bias, clamp, store of V accumulators as one LB-byte piece; max z per row.
+// Bias, clamp, store of V accumulators as one LB-byte piece; per row the max
+// z and the min |z - 16|.
 template <typename T, int LB>
-__device__ __forceinline__ void cc_store(float *acc, float *zmax, float bias, T *dst) {
+__device__ __forceinline__ void cc_store(float *acc, float *zmax, float *zdist, float bias, T *dst) {
     constexpr int V = LB / (int)sizeof(T);
     __align__(16) T ov[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
         const float z = acc[v] + bias;
         zmax[v] = fmaxf(zmax[v], z);
+        zdist[v] = fminf(zdist[v], fabsf(z - 16.0f));
         ov[v] = act_traits<T>::from_f(clamp32(z));
         acc[v] = 0.0f;
     }
@@ -248,7 +251,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     constexpr int ES = (int)sizeof(T), V = LB / ES, kWarps = NT / 32;
     constexpr int EB = 4 * cc_epv<T>();  // entries per block
     extern __shared__ uint4 cc_smem[];
-    __shared__ uint32_t s_zmax[kCcMaxTR];
+    __shared__ uint32_t s_zmax[kCcMaxTR], s_zdist[kCcMaxTR];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grid = (int)gridDim.x;
     int64_t total = 0;
@@ -283,7 +286,10 @@ __global__ void __launch_bounds__(NT, 512 / NT)
                 for (int k = 0; k < 8; ++k) cc_smem[i + k * NT] = v[k];
             }
             for (; i < nvec; i += NT) cc_smem[i] = __ldg(src + i);
-            for (int r = threadIdx.x; r < TR; r += NT) s_zmax[r] = 0u;
+            for (int r = threadIdx.x; r < TR; r += NT) {
+                s_zmax[r] = 0u;
+                s_zdist[r] = 0x7F800000u;  // +inf
+            }
         }
         if (threadIdx.x == 0 && item + grid < total) {
             // the next tile of this CTA into L2 while this one is computed
@@ -313,11 +319,12 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         const int j0 = j_lo + warp * opw + o;
         const int nout = j0 < j_hi ? (j_hi - j0 + step - 1) / step : 0;
         const int nsteps = nout * nb;
-        float acc[V], zmax[V];
+        float acc[V], zmax[V], zdist[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             acc[v] = 0.0f;
             zmax[v] = -INFINITY;
+            zdist[v] = INFINITY;
         }
         int jl = j0, bl = 0, jc = j0, bc = 0;
         uint4 qa[4], qb[4], qc[4];
@@ -330,7 +337,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         };
         auto finish_step = [&]() {
             if (++bc == nb) {
-                cc_store<T, LB>(acc, zmax, bias, out + ((int64_t)it.tile * N + jc) * TR + c * V);
+                cc_store<T, LB>(acc, zmax, zdist, bias, out + ((int64_t)it.tile * N + jc) * TR + c * V);
                 bc = 0;
                 jc += step;
             }
@@ -355,20 +362,25 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         // the row's error bound, max output and output error
 #pragma unroll
         for (int v = 0; v < V; ++v)
-            for (int off = G; off < 32; off <<= 1) zmax[v] = fmaxf(zmax[v], __shfl_xor_sync(0xffffffffu, zmax[v], off));
+            for (int off = G; off < 32; off <<= 1) {
+                zmax[v] = fmaxf(zmax[v], __shfl_xor_sync(0xffffffffu, zmax[v], off));
+                zdist[v] = fminf(zdist[v], __shfl_xor_sync(0xffffffffu, zdist[v], off));
+            }
         if (o == 0) {
 #pragma unroll
-            for (int v = 0; v < V; ++v) atomicMax(&s_zmax[c * V + v], f2ord(zmax[v]));
+            for (int v = 0; v < V; ++v) {
+                atomicMax(&s_zmax[c * V + v], f2ord(zmax[v]));
+                atomicMin(&s_zdist[c * V + v], __float_as_uint(zdist[v]));  // >= 0: bit order = value order
+            }
         }
         __syncthreads();
         const double steps = fast_steps(nd, lw);
         for (int r = threadIdx.x; r < TR; r += NT) {
             const int p = it.tile * TR + r;
             if (p < R) {
-                const float zm = ord2f(s_zmax[r]);
                 const float ez = z_error_bound(nd.err[par][p], nd.mx[par][p], lw.S, lw.dW, bias, steps);
                 float em, ym;
-                row_stats<T>(zm, ez, em, ym);
+                row_stats<T>(ord2f(s_zmax[r]), __uint_as_float(s_zdist[r]), ez, em, ym);
                 atomicMax(&nd.stat[3 * p], s_zmax[r]);
                 atomicMax(&nd.stat[3 * p + 1], __float_as_uint(em));
                 atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));

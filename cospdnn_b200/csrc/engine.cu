@@ -717,6 +717,38 @@ extern "C" int cospdnn_engine_run(cospdnn_engine *e, void *stream) {
     return COSPDNN_OK;
 }
 
+extern "C" int cospdnn_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+extern "C" int cospdnn_engine_run_timed(cospdnn_engine *e, void *stream, float *ms) {
+    CSP_CHECK(e && ms, COSPDNN_ERR_INVALID, "run_timed: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "run_timed: build first");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t a, b;
+    CSP_CUDA(cudaEventCreate(&a));
+    cudaError_t err = cudaEventCreate(&b);
+    if (err != cudaSuccess) {
+        cudaEventDestroy(a);
+        return cuda_fail(err, "run_timed: event");
+    }
+    err = cudaEventRecord(a, s);
+    if (err == cudaSuccess) err = cudaGraphLaunch(e->exec, s);
+    if (err == cudaSuccess) err = cudaEventRecord(b, s);
+    if (err == cudaSuccess) err = cudaEventSynchronize(b);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CSP_CUDA(err);
+    return COSPDNN_OK;
+}
+
 extern "C" int cospdnn_engine_result(cospdnn_engine *e, int net, int32_t *categories, int64_t *count,
                                      int64_t *alive_per_layer, int64_t *rechecked_per_layer,
                                      void *stream) {

@@ -164,8 +164,17 @@ int cospdnn_engine_build(cospdnn_engine *e);
  * Asynchronous on `stream`. */
 int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *y0, int format,
                              int on_device, void *stream);
+/* Number of CUDA devices visible to this process (0 when none, or on error);
+ * replaces cudaGetDeviceCount in the reference's multi-GPU launcher
+ * (src/cospdnn.cpp:155-163). */
+int cospdnn_device_count(void);
 /* Runs every network to completion: one graph launch, asynchronous. */
 int cospdnn_engine_run(cospdnn_engine *e, void *stream);
+/* cospdnn_engine_run bracketed by CUDA events on `stream`; waits for the run
+ * and returns its device time in *ms.  Replaces the event timing around the
+ * reference's layer loop that prints "Kernel Exec Time" (src/cospdnn.cu:303-310,
+ * src/cospdnn_double.cu:1142). */
+int cospdnn_engine_run_timed(cospdnn_engine *e, void *stream, float *ms);
 /* Synchronizes `stream`, then copies results of one network to host memory:
  * categories (ascending original row ids, room for `rows`), their count,
  * alive rows after each layer (room for `layers`, may be NULL) and rows

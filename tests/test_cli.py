@@ -1,0 +1,85 @@
+"""The reference's command lines, rebuilt over the C ABI
+(cospdnn_b200/cli/cospdnn.out and cospdnn_double.out): argv, dataset files
+(src/cospdnn.cpp:13-79) and the per-layer survivor lines, checked against the
+FP64 oracle on a dataset written in the reference's formats with a
+non-trivial fuse permutation."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from netgen import make_net, oracle_run
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "cospdnn_b200", "cli")
+
+
+def _exe(name):
+    p = os.path.join(CLI, name + ".out")
+    if not os.path.exists(p):
+        pytest.skip("command lines not built (python -m cospdnn_b200.build)")
+    return p
+
+
+@pytest.mark.parametrize("name,nargs", [("cospdnn", 6), ("cospdnn_double", 8)])
+def test_cli_usage(name, nargs):
+    out = subprocess.run([_exe(name)] + ["1"] * (nargs - 1), capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0
+    assert out.stdout.startswith("Usage: exe neuron")
+
+
+def _dataset(tmp, n, L, rows, seed, net):
+    """Writes a net in the reference's formats with a random fuse per layer and
+    returns the oracle's view (weights folded through the fuse)."""
+    from cospdnn_b200 import synth
+    from oracle import pyoracle as po
+    csc, y0, b = make_net(n, L, rows, seed=seed, net=net, dlo=0.2, dhi=0.4)
+    rng = np.random.default_rng(seed)
+    fuse = [rng.permutation(n).astype(np.int32) for _ in range(L)]
+    synth.write_reference_dataset(str(tmp), n, L, y0, csc, fuse=fuse)
+    folded = []
+    for l, (cp, ri, vv) in enumerate(csc):
+        row, col, val = po.csc_to_coo(cp, ri, vv)
+        folded.append(po.coo_to_csc(fuse[l][row], col, val, n))
+    return oracle_run(folded, y0, b)
+
+
+def _alive(text, prefix):
+    pat = re.compile(prefix + r"layer (\d+), feature = (\d+)")
+    got = {}
+    for m in pat.finditer(text):
+        got[int(m.group(1))] = int(m.group(2))
+    return [got[k] for k in sorted(got)]
+
+
+@pytest.mark.gpu
+def test_cli_single_matches_oracle(tmp_path):
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ref = _dataset(tmp_path, 1024, 6, 500, 43, 0)
+    for prec in ("fp16", "fp32"):
+        env = dict(os.environ, COSPDNN_PRECISION=prec)
+        out = subprocess.run([_exe("cospdnn"), "1024", "500", "6", "1", "0", str(tmp_path)],
+                             capture_output=True, text=True, timeout=600, env=env)
+        assert out.returncode == 0, out.stdout + out.stderr
+        assert _alive(out.stdout, "") == list(ref["alive"])
+        assert "Kernel Exec Time = " in out.stdout
+        assert f"[Categories] :{len(ref['categories'])}" in out.stdout
+
+
+@pytest.mark.gpu
+def test_cli_double_matches_oracle(tmp_path):
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ref1 = _dataset(tmp_path, 1024, 5, 400, 47, 0)
+    ref2 = _dataset(tmp_path, 2048, 7, 300, 53, 1)
+    out = subprocess.run([_exe("cospdnn_double"), "1024", "400", "5", "2048", "300", "7", "0", str(tmp_path)],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert _alive(out.stdout, "SpDNN 1 ") == list(ref1["alive"])
+    assert _alive(out.stdout, "SpDNN 2 ") == list(ref2["alive"])
+    assert "Total Kernel Exec Time = " in out.stdout
