@@ -275,9 +275,8 @@ def main():
     def max_over_ranks(x):
         if world == 1:
             return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from cospdnn_b200 import dist as cd
+        return cd.max_over_ranks(x, device=f"cuda:{local}")
 
     # ---- device-resident timing
     for _ in range(args.warmup):
