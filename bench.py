@@ -47,14 +47,23 @@ def config_nets(name):
         return synth.mix_config(SEED), "fp16", (0.08, 0.25)
     if name == "s1":
         return [(1024, 120, 60000)], "fp16", (0.25, 0.45)
+    if name == "r1":
+        return [(4096, 120, 60000)], "fp16", (0.08, 0.25)
     raise SystemExit(f"unknown config {name}")
+
+
+def weight_kind(name):
+    """r1: reference-compatible masks (two aligned dense 16x16 blocks per
+    block column, the structure the reference's kernel expects); else XOR."""
+    return "r1" if name == "r1" else "xor"
 
 
 def workload_name(name, nets, prec, dens):
     if len(nets) == 1:
         n, l, b = nets[0]
-        return (f"{n} neurons x {l} layers, {b} rows, XOR-mask W (32 nnz/col, 1/16), "
-                f"binary Y0 density U[{dens[0]},{dens[1]}], {prec}")
+        w = ("R1 W (two dense 16x16 blocks per block column, 32 nnz/col, 1/16)" if weight_kind(name) == "r1"
+             else "XOR-mask W (32 nnz/col, 1/16)")
+        return f"{n} neurons x {l} layers, {b} rows, {w}, binary Y0 density U[{dens[0]},{dens[1]}], {prec}"
     return (f"{len(nets)} networks {[(n, l, b) for n, l, b in nets]}, XOR-mask W, "
             f"binary Y0 density U[{dens[0]},{dens[1]}], {prec}")
 
@@ -141,14 +150,14 @@ def sample_rows(run, total, budget_s):
         rows = int(min(total, rows * max(2.0, min(8.0, 0.8 * budget_s / max(dt, 1e-3)))))
 
 
-def cpu_baseline(nets, dens, y0_host_fn, budget_s=12.0, threads=None):
+def cpu_baseline(nets, dens, y0_host_fn, budget_s=12.0, threads=None, kind="xor"):
     """Multithreaded FP32 CSR recurrence (oracle/ port) on a bounded row sample."""
     from cospdnn_b200 import synth
     from oracle import pyoracle as po
     threads = threads or os.cpu_count()
     total_edges, total_t, desc = 0.0, 0.0, []
     for i, (n, L, b) in enumerate(nets):
-        csr = [po.coo_to_csr(*po.csc_to_coo(*c), n) for c in synth.network(n, L, SEED, net=i)]
+        csr = [po.coo_to_csr(*po.csc_to_coo(*c), n) for c in synth.network(n, L, SEED, net=i, kind=kind)]
         bias = np.float32({1024: -0.3, 4096: -0.35, 16384: -0.4, 65536: -0.45}[n])
         rows = sample_rows(lambda r: po.infer_fp32_csr(csr, y0_host_fn(i, r), bias, threads=threads),
                            b, budget_s / len(nets))
@@ -175,7 +184,8 @@ def run_reference(args, nets, prec, dens):
     def host_rows(i, rows):
         return po.input_binary(SEED, i, rows, nets[i][0], dens[0], dens[1])
 
-    layers = [[po.coo_to_csr(*po.csc_to_coo(*c), n) for c in synth.network(n, L, SEED, net=i)]
+    layers = [[po.coo_to_csr(*po.csc_to_coo(*c), n) for c in synth.network(n, L, SEED, net=i,
+                                                                         kind=weight_kind(args.config))]
               for i, (n, L, b) in enumerate(nets)]
     # size one step to a bounded sample: ~budget seconds per step
     budget = max(2.0, 60.0 / max(1, args.steps + args.warmup))
@@ -254,7 +264,7 @@ def main():
     ids, inputs = [], []
     for i, (n, L, b) in enumerate(nets):
         nid = eng.add_net(n, L, b, cs.BIAS[n], cs.THRESHOLD, PREC[prec], args.kernel)
-        for l, (cp, ri, vv) in enumerate(synth.network(n, L, SEED, net=i)):
+        for l, (cp, ri, vv) in enumerate(synth.network(n, L, SEED, net=i, kind=weight_kind(args.config))):
             eng.set_layer_csc(nid, l, cp, ri, vv)
         ids.append(nid)
     eng.build()
@@ -371,7 +381,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(nets, dens, lambda i, rows: inputs[i][:rows].cpu().numpy())
+        cpu = cpu_baseline(nets, dens, lambda i, rows: inputs[i][:rows].cpu().numpy(), kind=weight_kind(args.config))
 
     clocks = clk.summary()
     if rank == 0:

@@ -92,9 +92,84 @@ __global__ void k_convert_tile(const uint8_t *__restrict__ src, int rows, int N,
             } else if (RC * (int)sizeof(T) == 32) {
                 reinterpret_cast<uint4 *>(dst)[0] = reinterpret_cast<const uint4 *>(o)[0];
                 reinterpret_cast<uint4 *>(dst)[1] = reinterpret_cast<const uint4 *>(o)[1];
+            } else if (RC * (int)sizeof(T) == 8) {
+                *reinterpret_cast<uint2 *>(dst) = *reinterpret_cast<const uint2 *>(o);
             } else {
                 for (int r = 0; r < RC; ++r) dst[r] = o[r];
             }
+        }
+    }
+}
+
+// Integer inputs (bytes or bits) into row-major buffers: one thread per
+// (row, 8 features), one 16-byte piece (two for FP32) per thread.
+template <typename T, int FMT>
+__global__ void k_convert_pieces(const uint8_t *__restrict__ src, int rows, int N, int layout,
+                                 T *__restrict__ y0) {
+    const int nfb = N / 8;
+    const int64_t total = (int64_t)rows * nfb;
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = u / nfb;
+        const int fb = (int)(u - row * nfb);
+        uint2 b;
+        if (FMT == COSPDNN_INPUT_U8) {
+            b = *reinterpret_cast<const uint2 *>(src + row * N + 8 * fb);
+        } else {
+            const uint32_t bits = src[row * nfb + fb];
+            b.x = (bits & 1u) | ((bits >> 1) & 1u) << 8 | ((bits >> 2) & 1u) << 16 | ((bits >> 3) & 1u) << 24;
+            b.y = ((bits >> 4) & 1u) | ((bits >> 5) & 1u) << 8 | ((bits >> 6) & 1u) << 16 | ((bits >> 7) & 1u) << 24;
+        }
+        __align__(16) T o[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            o[k] = act_traits<T>::from_f((float)((b.x >> (8 * k)) & 0xFFu));
+            o[k + 4] = act_traits<T>::from_f((float)((b.y >> (8 * k)) & 0xFFu));
+        }
+        T *dst = y0 + act_index(layout, N, row, 8 * fb);
+        reinterpret_cast<uint4 *>(dst)[0] = reinterpret_cast<const uint4 *>(o)[0];
+        if (sizeof(T) == 4) reinterpret_cast<uint4 *>(dst)[1] = reinterpret_cast<const uint4 *>(o)[1];
+    }
+}
+
+// Integer inputs into MMA tiles (layout 1): one CTA (256 threads) per
+// (128-row tile, 64 features); the slab is staged in shared memory as bytes,
+// then every 16-feature block is written as one contiguous 4 KB operand.
+template <typename T, int FMT>
+__global__ void __launch_bounds__(256) k_convert_mma(const uint8_t *__restrict__ src, int rows, int N,
+                                                     T *__restrict__ y0) {
+    __shared__ __align__(16) uint8_t slab[128][64];
+    const int ng = (N + 63) / 64, nbk = N / 16;
+    const int64_t units = (int64_t)((rows + 127) / 128) * ng;
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const int64_t t = u / ng;
+        const int g = (int)(u - t * ng), fw = min(64, N - 64 * g);
+        __syncthreads();  // the previous unit is done with the slab
+        if (FMT == COSPDNN_INPUT_U8) {
+            for (int i = threadIdx.x; i < 128 * 4; i += 256) {  // 16-byte pieces
+                const int m = i >> 2, pc = i & 3;
+                const int64_t row = t * 128 + m;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (row < rows && pc * 16 < fw) v = *reinterpret_cast<const uint4 *>(src + row * N + 64 * g + 16 * pc);
+                *reinterpret_cast<uint4 *>(&slab[m][16 * pc]) = v;
+            }
+        } else {
+            for (int i = threadIdx.x; i < 128 * 8; i += 256) {  // bytes of 8 features
+                const int m = i >> 3, by = i & 7;
+                const int64_t row = t * 128 + m;
+                const uint32_t bits = (row < rows && by * 8 < fw) ? src[row * (N / 8) + 8 * g + by] : 0u;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) slab[m][8 * by + k] = (uint8_t)((bits >> k) & 1u);
+            }
+        }
+        __syncthreads();
+        for (int b = 0; b < fw / 16; ++b) {
+            // piece i of the block: rows m, 8-feature half kh (canonical order)
+            const int i = threadIdx.x, m = ((i >> 4) << 3) + (i & 7), kh = (i >> 3) & 1;
+            __align__(16) T o[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) o[k] = act_traits<T>::from_f((float)slab[m][16 * b + 8 * kh + k]);
+            T *dst = y0 + ((t * nbk) + 4 * g + b) * 2048 + (int64_t)i * 8;
+            *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(o);
         }
     }
 }
@@ -239,6 +314,44 @@ struct DeviceGuard {
         if (prev >= 0 && cur != prev) cudaSetDevice(prev);
     }
 };
+
+// Fraction of the 16x16 aligned blocks of W that its nonzeros fill, over all
+// layers (1 = every touched block dense; XOR-mask weights: 1/16).
+double block_fill(const Net &net) {
+    const int N = net.d.neuron, nb = (N + 15) / 16;
+    double nnz = 0.0, blocks = 0.0;
+    std::vector<int> mark(nb, -1);
+    for (const HostLayer &h : net.layers) {
+        nnz += h.colptr[N];
+        for (int c = 0; c < nb; ++c) {  // block column c: distinct input blocks
+            for (int j = c * 16; j < std::min(N, c * 16 + 16); ++j)
+                for (int p = h.colptr[j]; p < h.colptr[j + 1]; ++p) {
+                    const int b = h.rowidx[p] / 16;
+                    if (mark[b] != c) {
+                        mark[b] = c;
+                        blocks += 1.0;
+                    }
+                }
+        }
+        std::fill(mark.begin(), mark.end(), -1);
+    }
+    return blocks > 0.0 ? nnz / (blocks * 256.0) : 0.0;
+}
+
+// Kernel for COSPDNN_KERNEL_AUTO.  The CUDA-core row-tile kernel costs about
+// the same per nonzero whatever the sparsity pattern; a tcgen05 MMA costs a
+// fixed 16x16 block whatever its fill.  Measured on one B200 (4096 neurons,
+// 60000 rows, FP16): one layer takes 0.86 ms on CUDA cores for any pattern,
+// 2.13 ms on tcgen05 at 29 blocks per block column (fill 1/16, XOR masks) and
+// 0.39 ms at 2 (fill 1); the lines cross near 9.5 blocks, fill 0.21.  So
+// tcgen05 when its blocks are at least a quarter full or when the row tile
+// of the CUDA-core kernel does not fit; FP32 always on CUDA cores.
+int auto_kernel(const Net &n) {
+    const int N = n.d.neuron, prec = n.d.precision;
+    if (prec == COSPDNN_PREC_FP32 || !tc_supported(N)) return COSPDNN_KERNEL_CUDA_CORE;
+    if (cc_tile_rows(N, prec) == 0) return COSPDNN_KERNEL_TCGEN05;
+    return block_fill(n) >= 0.25 ? COSPDNN_KERNEL_TCGEN05 : COSPDNN_KERNEL_CUDA_CORE;
+}
 
 int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
     const HostLayer &h = net.layers[l];
@@ -432,15 +545,10 @@ extern "C" int cospdnn_engine_add_net(cospdnn_engine *e, const cospdnn_net_desc 
     Net net;
     net.d = *d;
     net.layers.resize(d->layers);
-    int k = d->kernel;
-    if (k == COSPDNN_KERNEL_AUTO)
-        k = (cc_tile_rows(d->neuron, d->precision) == 0 && d->precision != COSPDNN_PREC_FP32 &&
-             tc_supported(d->neuron))
-                ? COSPDNN_KERNEL_TCGEN05
-                : COSPDNN_KERNEL_CUDA_CORE;
+    const int k = d->kernel;
     if (k == COSPDNN_KERNEL_TCGEN05)
         CSP_CHECK(tc_supported(d->neuron), COSPDNN_ERR_UNSUPPORTED, "add_net: tcgen05 kernel needs neuron % 16 == 0");
-    net.dev.kernel = k;
+    net.dev.kernel = k;  // AUTO is resolved at build, from the weights
     e->nets.push_back(std::move(net));
     if (net_id) *net_id = (int)e->nets.size() - 1;
     return COSPDNN_OK;
@@ -531,6 +639,7 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     for (Net &n : e->nets) {
         for (int l = 0; l < n.d.layers; ++l)
             CSP_CHECK(n.layers[l].set, COSPDNN_ERR_STATE, "build: a layer's weights were not set");
+        if (n.dev.kernel == COSPDNN_KERNEL_AUTO) n.dev.kernel = auto_kernel(n);
         e->max_n = std::max(e->max_n, n.d.neuron);
         e->max_layers = std::max(e->max_layers, n.d.layers);
         // activation layout: MMA tiles (tcgen05), row tiles (CUDA-core tile
@@ -678,6 +787,33 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     }
     const int blocks = std::min(65535, (R + 7) / 8);
     float *err0 = (float *)n.dev.err0, *mx0 = (float *)n.dev.mx0;
+    if (n.dev.layout < 2 && format != COSPDNN_INPUT_F32) {
+        // integer input into row-major or MMA-tile buffers
+        const uint8_t *b = (const uint8_t *)src;
+        const int64_t units = (int64_t)R * (N / 8);
+        const int cb = (int)std::min<int64_t>((units + 255) / 256, 148 * 16);
+        const int layout = n.dev.layout;
+        const int mb = (int)std::min<int64_t>((int64_t)((R + 127) / 128) * ((N + 63) / 64), 148 * 8);
+#define CSP_PIECES(T)                                                                                        \
+    do {                                                                                                     \
+        if (layout == 1) {                                                                                   \
+            if (format == COSPDNN_INPUT_U8) k_convert_mma<T, COSPDNN_INPUT_U8><<<mb, 256, 0, s>>>(b, R, N, (T *)n.dev.y0); \
+            else k_convert_mma<T, COSPDNN_INPUT_BITS><<<mb, 256, 0, s>>>(b, R, N, (T *)n.dev.y0);                \
+        } else if (format == COSPDNN_INPUT_U8) {                                                             \
+            k_convert_pieces<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)n.dev.y0);        \
+        } else {                                                                                             \
+            k_convert_pieces<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)n.dev.y0);      \
+        }                                                                                                    \
+    } while (0)
+        if (n.d.precision == COSPDNN_PREC_FP32) CSP_PIECES(float);
+        else if (n.d.precision == COSPDNN_PREC_FP16) CSP_PIECES(__half);
+        else CSP_PIECES(__nv_bfloat16);
+#undef CSP_PIECES
+        if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
+        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
+        CSP_CUDA(cudaGetLastError());
+        return COSPDNN_OK;
+    }
     if (n.dev.layout >= 2 && format != COSPDNN_INPUT_F32) {
         // integer input into row tiles
         const uint8_t *b = (const uint8_t *)src;

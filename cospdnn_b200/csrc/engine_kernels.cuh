@@ -559,36 +559,34 @@ __global__ void __launch_bounds__(kCopyThreads)
     __shared__ uint4 stage[kCopyStageBytes / 16];
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
-    int64_t total = 0, tiles = 0;
+    int64_t rows_total = 0, tiles = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (nd.layout >= 2) {
-            tiles += (int64_t)((nd.st->copy_R + nd.layout - 1) / nd.layout) * copy_chunks(nd, gridDim.x);
-            continue;
-        }
-        const int es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2;
-        total += (int64_t)nd.st->copy_R * (nd.N * es / 16);
+        if (nd.layout >= 2) tiles += (int64_t)((nd.st->copy_R + nd.layout - 1) / nd.layout) * copy_chunks(nd, gridDim.x);
+        else rows_total += nd.st->copy_R;
     }
-    for (int64_t i = tid; i < total; i += nth) {
-        int64_t u = i;
+    // row-major and MMA-tile nets: one warp per kept row, lanes over its
+    // 16-byte pieces (8 features for 16-bit types, 4 for FP32)
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = tid >> 5, nw = nth >> 5;
+    for (int64_t w = gw; w < rows_total; w += nw) {
+        int64_t u = w;
         int n = 0;
-        int es = 4, pieces = 1;
         for (; n < nnets; ++n) {
             if (nets[n].layout >= 2) continue;
-            es = nets[n].prec == COSPDNN_PREC_FP32 ? 4 : 2;
-            pieces = nets[n].N * es / 16;
-            const int64_t cnt = (int64_t)nets[n].st->copy_R * pieces;
-            if (u < cnt) break;
-            u -= cnt;
+            if (u < nets[n].st->copy_R) break;
+            u -= nets[n].st->copy_R;
         }
         const NetDev &nd = nets[n];
-        const int N = nd.N, ib = nd.st->in_buf, per = 16 / es;
-        const int q = (int)(u / pieces), f = (int)(u % pieces) * per;
+        const int N = nd.N, ib = nd.st->in_buf, q = (int)u;
+        const int es = nd.prec == COSPDNN_PREC_FP32 ? 4 : 2, per = 16 / es;
         const int p = nd.cmap[q];
         const char *src = (const char *)nd.act[ib ^ 1];
         char *dst = (char *)nd.act[ib];
-        const uint4 v = *reinterpret_cast<const uint4 *>(src + act_index(nd.layout, N, p, f) * es);
-        *reinterpret_cast<uint4 *>(dst + act_index(nd.layout, N, q, f) * es) = v;
+        for (int f = lane * per; f < N; f += 32 * per) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(src + act_index(nd.layout, N, p, f) * es);
+            *reinterpret_cast<uint4 *>(dst + act_index(nd.layout, N, q, f) * es) = v;
+        }
     }
     // row-tile nets: items of (destination tile, feature chunk)
     for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {

@@ -125,7 +125,9 @@ typedef struct cospdnn_engine cospdnn_engine;
 #define COSPDNN_PREC_FP16 1 /* FP16 activations, FP32 accumulation */
 #define COSPDNN_PREC_BF16 2 /* BF16 activations, FP32 accumulation */
 
-#define COSPDNN_KERNEL_AUTO 0      /* tensor cores for FP16/BF16, CUDA cores for FP32 */
+#define COSPDNN_KERNEL_AUTO 0      /* chosen at build from the weights: tcgen05 for FP16/BF16 when the
+                                      16x16 blocks are at least 1/4 full or the row tile does not fit
+                                      shared memory, else CUDA cores; FP32 on CUDA cores */
 #define COSPDNN_KERNEL_CUDA_CORE 1 /* gather-FMA kernel, any precision */
 #define COSPDNN_KERNEL_TCGEN05 2   /* tcgen05 block MMA kernel (FP16/BF16) */
 

@@ -18,7 +18,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libref_cospdnn.so")
 
 
-def run_reference_loop(oracle, csc, y0, bias):
+def run_reference_loop(oracle, csc, y0, bias, want_wall=False):
     ref = C.CDLL(REF_SO)
     L, n = len(csc), y0.shape[1]
     vals, rows, ptrs = [], [], []
@@ -50,6 +50,8 @@ def run_reference_loop(oracle, csc, y0, bias):
                              float(bias), C.addressof(kms), C.addressof(wms), C.addressof(last),
                              feats.ctypes.data, 64, tail, 4096)
     assert rc == 0, tail.value.decode()
+    if want_wall:
+        return feats, kms.value, wms.value
     return feats, kms.value
 
 
