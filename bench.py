@@ -72,6 +72,17 @@ def edges(nets):
     return float(sum(b * l * 32 * n for n, l, b in nets))
 
 
+# DRAM bytes (read + write) per input row of one layer launch of the
+# dominant kernel, from one ncu capture of a smaller case of the same
+# workload (profiles/k_layer_*.md): traffic grows with the rows processed.
+DRAM_BYTES_PER_ROW = {
+    "c2": (135.131136e6 + 88.350208e6) / 16384,  # k_layer_cc_4096n_16384rows_fp16.md
+    "c1": (135.193088e6 + 88.413696e6) / 32768,  # k_layer_cc_1024n_32768rows_fp32.md
+    "c3": (271.177216e6 + 224.850688e6) / 8192,  # k_layer_cc_16384n_8192rows_bf16.md
+    "r1": (134.869248e6 + 83.793152e6) / 16384,  # k_layer_tc_4096n_16384rows_r1_fp16.md
+}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -330,9 +341,18 @@ def main():
     peak, peak_kind = measured_peaks()
     tot_b, tot_t = float(layer_bytes.sum()), float(lms[:nit].sum()) * 1e-3
     achieved = tot_b / tot_t / 1e9 if tot_t > 0 else 0.0
+    rows_per_launch = 0.0
+    for r, (n, L, b) in zip(results, nets):
+        rows_in = np.concatenate([[b], r["alive"][:-1]])
+        rows_per_launch += float(rows_in[:min(nit, L)].sum()) / max(1, nit)
+    traffic = None
+    if args.config in DRAM_BYTES_PER_ROW and args.precision in (None, prec) and args.kernel == 0:
+        traffic = DRAM_BYTES_PER_ROW[args.config] * rows_per_launch
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                "kernel": "layer kernel (k_layer_plain / tc layer)",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "layer kernel of the net (row-tile CUDA-core, tcgen05 or row-major gather)",
+                "traffic_note": "DRAM bytes per launch scaled from an ncu capture of a smaller case "
+                                "(per input row) to this workload's average rows per layer launch",
                 "bytes_per_launch": tot_b / max(1, nit),
                 "ms_per_launch": float(lms[:nit].mean()) if nit else 0.0,
                 "per_layer": per_layer[:8]}
