@@ -240,3 +240,48 @@ def test_engine_input_formats_agree(cs, n, prec, kernel):
     for r, f in outs:
         check_parity(r, ref, 4)
         np.testing.assert_array_equal(f, outs[0][1])
+
+
+def _empty_columns_layer(n, seed):
+    """Random weights where a quarter of the outputs have no inputs at all."""
+    from netgen import random_layer
+    cp, ri, vv = random_layer(n, seed, 0)
+    rng = np.random.default_rng(seed)
+    empty = rng.random(n) < 0.25
+    keep = np.repeat(~empty, np.diff(cp))
+    counts = np.where(empty, 0, np.diff(cp))
+    return np.concatenate([[0], np.cumsum(counts)]).astype(np.int32), ri[keep], vv[keep]
+
+
+@pytest.mark.parametrize("prec,kernel", [(1, 1), (0, 1), (1, 2)])
+def test_engine_edge_cases(cs, prec, kernel):
+    """In one engine: a net with no rows, a one-layer net, a net whose layers
+    have outputs without inputs, and a net whose second layer has no weights
+    at all (every row pruned there)."""
+    from netgen import make_random_net
+    n = 1024
+    c_a, y_a, b_a = make_random_net(n, 3, 200, seed=71)
+    c_b, y_b, b_b = make_random_net(n, 1, 150, seed=72)
+    c_c = [_empty_columns_layer(n, 73 + l) for l in range(4)]
+    _, y_c, b_c = make_random_net(n, 1, 250, seed=73)
+    c_d, y_d, b_d = make_random_net(n, 3, 120, seed=74)
+    c_d[1] = (np.zeros(n + 1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32))
+    nets = [(c_a, y_a[:0], b_a), (c_b, y_b, b_b), (c_c, y_c, b_c), (c_d, y_d, b_d)]
+    eng = cs.Engine(0)
+    ids = []
+    for csc, y0, b in nets:
+        nid = eng.add_net(n, len(csc), y0.shape[0], float(b), 1e-5, prec, kernel)
+        for l, (cp, ri, vv) in enumerate(csc):
+            eng.set_layer_csc(nid, l, cp, ri, vv)
+        ids.append(nid)
+    eng.build()
+    for nid, (_, y0, _) in zip(ids, nets):
+        if y0.shape[0]:
+            eng.set_input(nid, y0)
+    eng.run()
+    res = [eng.result(nid) for nid in ids]
+    eng.close()
+    assert len(res[0]["categories"]) == 0
+    for r, (csc, y0, b) in zip(res[1:], nets[1:]):
+        check_parity(r, oracle_run(csc, y0, b), len(csc))
+    assert res[3]["alive"][1] == 0 and len(res[3]["categories"]) == 0
