@@ -247,9 +247,18 @@ struct Net {
     NetDev dev{};
     std::vector<LayerDev> ldev;
     LayerDev *d_layers = nullptr;
-    void *staging = nullptr;
-    size_t staging_bytes = 0;
-    float *y0_f32 = nullptr;
+    // Inputs are double buffered: set_input fills the back buffers (staging
+    // copy, Y0 in the compute type, per-row error and max, exact FP32 rows),
+    // the next run makes them current.  So the copy and conversion of the
+    // next batch can run on another stream while a run reads the current one.
+    void *staging[2] = {nullptr, nullptr};
+    size_t staging_bytes[2] = {0, 0};
+    void *y0buf[2] = {nullptr, nullptr};
+    float *err0buf[2] = {nullptr, nullptr}, *mx0buf[2] = {nullptr, nullptr};
+    float *f32buf[2] = {nullptr, nullptr};  // exact rows of FP32 inputs (allocated on first use)
+    bool f32used[2] = {false, false};       // the buffer's last input came as FP32
+    int front = 0;                          // buffers of the current input
+    bool pending = false;                   // the back buffers hold a newer input
 };
 
 }  // namespace
@@ -678,10 +687,20 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         d.layers = n.d_layers;
         const size_t rows_pad = (size_t)(R + 127) / 128 * 128;
         const size_t es = elem_size(d.prec), act = rows_pad * N * es;
-        d.y0 = dalloc<char>(act, e->owned);
+        for (int b = 0; b < 2; ++b) {
+            n.y0buf[b] = dalloc<char>(act, e->owned);
+            n.err0buf[b] = dalloc<float>(R, e->owned);
+            n.mx0buf[b] = dalloc<float>(R, e->owned);
+            CSP_CHECK(n.y0buf[b] && n.err0buf[b] && n.mx0buf[b], COSPDNN_ERR_NOMEM, "build: device allocation failed");
+            CSP_CUDA(cudaMemset(n.y0buf[b], 0, act));
+            CSP_CUDA(cudaMemset(n.err0buf[b], 0, sizeof(float) * R));
+            CSP_CUDA(cudaMemset(n.mx0buf[b], 0, sizeof(float) * R));
+        }
+        n.front = 0;
+        d.y0 = n.y0buf[0];
         d.act[0] = dalloc<char>(act, e->owned);
         d.act[1] = dalloc<char>(act, e->owned);
-        float *err0 = dalloc<float>(R, e->owned), *mx0 = dalloc<float>(R, e->owned);
+        float *err0 = n.err0buf[0], *mx0 = n.mx0buf[0];
         d.err0 = err0;
         d.mx0 = mx0;
         d.cmap = dalloc<int32_t>(R, e->owned);
@@ -705,11 +724,8 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
                       d.orig[1] && d.err[0] && d.err[1] && d.mx[0] && d.mx[1] && d.stat && d.cls &&
                       d.ulist && d.alive_count && d.recheck_count && d.st,
                   COSPDNN_ERR_NOMEM, "build: device allocation failed");
-        CSP_CUDA(cudaMemset((void *)d.y0, 0, act));
         CSP_CUDA(cudaMemset(d.act[0], 0, act));
         CSP_CUDA(cudaMemset(d.act[1], 0, act));
-        CSP_CUDA(cudaMemset(err0, 0, sizeof(float) * R));
-        CSP_CUDA(cudaMemset(mx0, 0, sizeof(float) * R));
         CSP_CUDA(cudaMemset(d.st, 0, sizeof(NetState)));
     }
     for (Net &n : e->nets) {
@@ -755,38 +771,37 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     const size_t bytes = format == COSPDNN_INPUT_U8 ? (size_t)R * N
                        : format == COSPDNN_INPUT_F32 ? (size_t)R * N * 4 : (size_t)R * (N / 8);
     cudaStream_t s = (cudaStream_t)stream;
+    const int back = n.front ^ 1;  // the current input stays untouched for a run in flight
     const void *src = y0;
     if (!on_device) {
-        if (n.staging_bytes < bytes) {
-            if (n.staging) {
+        if (n.staging_bytes[back] < bytes) {
+            if (n.staging[back]) {
                 // the engine owns the old buffer: drop it from the list it frees at destruction
-                e->owned.erase(std::remove(e->owned.begin(), e->owned.end(), n.staging), e->owned.end());
-                cudaFree(n.staging);
+                e->owned.erase(std::remove(e->owned.begin(), e->owned.end(), n.staging[back]), e->owned.end());
+                cudaFree(n.staging[back]);
             }
-            n.staging = nullptr;
-            n.staging_bytes = 0;
-            CSP_CUDA(cudaMalloc(&n.staging, bytes));
-            e->owned.push_back(n.staging);
-            n.staging_bytes = bytes;
+            n.staging[back] = nullptr;
+            n.staging_bytes[back] = 0;
+            CSP_CUDA(cudaMalloc(&n.staging[back], bytes));
+            e->owned.push_back(n.staging[back]);
+            n.staging_bytes[back] = bytes;
         }
-        CSP_CUDA(cudaMemcpyAsync(n.staging, y0, bytes, cudaMemcpyHostToDevice, s));
-        src = n.staging;
+        CSP_CUDA(cudaMemcpyAsync(n.staging[back], y0, bytes, cudaMemcpyHostToDevice, s));
+        src = n.staging[back];
     }
     float *f32 = nullptr;
     if (format == COSPDNN_INPUT_F32 && n.d.precision != COSPDNN_PREC_FP32) {
-        if (!n.y0_f32) {
-            CSP_CUDA(cudaMalloc(&n.y0_f32, (size_t)R * N * 4));
-            e->owned.push_back(n.y0_f32);
+        if (!n.f32buf[back]) {
+            CSP_CUDA(cudaMalloc(&n.f32buf[back], (size_t)R * N * 4));
+            e->owned.push_back(n.f32buf[back]);
         }
-        f32 = n.y0_f32;
+        f32 = n.f32buf[back];
     }
-    if (n.dev.y0_f32 != f32) {
-        n.dev.y0_f32 = f32;
-        CSP_CUDA(cudaMemcpyAsync(&e->d_nets[net].y0_f32, &n.dev.y0_f32, sizeof(float *), cudaMemcpyHostToDevice, s));
-        CSP_CUDA(cudaStreamSynchronize(s));
-    }
+    n.f32used[back] = f32 != nullptr;
+    n.pending = true;
+    void *const y0dst = n.y0buf[back];
     const int blocks = std::min(65535, (R + 7) / 8);
-    float *err0 = (float *)n.dev.err0, *mx0 = (float *)n.dev.mx0;
+    float *err0 = n.err0buf[back], *mx0 = n.mx0buf[back];
     if (n.dev.layout < 2 && format != COSPDNN_INPUT_F32) {
         // integer input into row-major or MMA-tile buffers
         const uint8_t *b = (const uint8_t *)src;
@@ -797,12 +812,12 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
 #define CSP_PIECES(T)                                                                                        \
     do {                                                                                                     \
         if (layout == 1) {                                                                                   \
-            if (format == COSPDNN_INPUT_U8) k_convert_mma<T, COSPDNN_INPUT_U8><<<mb, 256, 0, s>>>(b, R, N, (T *)n.dev.y0); \
-            else k_convert_mma<T, COSPDNN_INPUT_BITS><<<mb, 256, 0, s>>>(b, R, N, (T *)n.dev.y0);                \
+            if (format == COSPDNN_INPUT_U8) k_convert_mma<T, COSPDNN_INPUT_U8><<<mb, 256, 0, s>>>(b, R, N, (T *)y0dst); \
+            else k_convert_mma<T, COSPDNN_INPUT_BITS><<<mb, 256, 0, s>>>(b, R, N, (T *)y0dst);                \
         } else if (format == COSPDNN_INPUT_U8) {                                                             \
-            k_convert_pieces<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)n.dev.y0);        \
+            k_convert_pieces<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)y0dst);        \
         } else {                                                                                             \
-            k_convert_pieces<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)n.dev.y0);      \
+            k_convert_pieces<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)y0dst);      \
         }                                                                                                    \
     } while (0)
         if (n.d.precision == COSPDNN_PREC_FP32) CSP_PIECES(float);
@@ -820,7 +835,7 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
         const int TR = n.dev.layout;
         const int64_t units = (int64_t)((R + TR - 1) / TR) * (TR / std::min(TR, 8)) * (N / 8);
         const int cb = (int)std::min<int64_t>((units + 255) / 256, 148 * 16);
-#define CSP_TILE(T)                                                                                             do {                                                                                                            if (format == COSPDNN_INPUT_U8) k_convert_tile<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)n.dev.y0);         else k_convert_tile<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)n.dev.y0);                } while (0)
+#define CSP_TILE(T)                                                                                             do {                                                                                                            if (format == COSPDNN_INPUT_U8) k_convert_tile<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)y0dst);         else k_convert_tile<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)y0dst);                } while (0)
         if (n.d.precision == COSPDNN_PREC_FP32) CSP_TILE(float);
         else if (n.d.precision == COSPDNN_PREC_FP16) CSP_TILE(__half);
         else CSP_TILE(__nv_bfloat16);
@@ -832,7 +847,7 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     }
 #define CSP_CONV(T)                                                                                      \
     do {                                                                                                 \
-        T *dst = (T *)n.dev.y0;                                                                          \
+        T *dst = (T *)y0dst;                                                                          \
         if (format == COSPDNN_INPUT_U8) k_convert_input<T, COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, R, N, n.dev.layout, dst, f32, err0, mx0); \
         else if (format == COSPDNN_INPUT_F32) k_convert_input<T, COSPDNN_INPUT_F32><<<blocks, 256, 0, s>>>(src, R, N, n.dev.layout, dst, f32, err0, mx0); \
         else k_convert_input<T, COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, R, N, n.dev.layout, dst, f32, err0, mx0); \
@@ -845,10 +860,35 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     return COSPDNN_OK;
 }
 
+namespace {
+
+// Makes the inputs set since the last run current: swaps each such net's
+// input buffers and updates its device descriptor, ordered on `s` before
+// the run that reads it.
+int take_inputs(cospdnn_engine *e, cudaStream_t s) {
+    for (size_t i = 0; i < e->nets.size(); ++i) {
+        Net &n = e->nets[i];
+        if (!n.pending) continue;
+        n.front ^= 1;
+        n.pending = false;
+        n.dev.y0 = n.y0buf[n.front];
+        n.dev.err0 = n.err0buf[n.front];
+        n.dev.mx0 = n.mx0buf[n.front];
+        n.dev.y0_f32 = n.f32used[n.front] ? n.f32buf[n.front] : nullptr;
+        // from pageable memory: the descriptor is staged before the call returns
+        CSP_CUDA(cudaMemcpyAsync(e->d_nets + i, &n.dev, sizeof(NetDev), cudaMemcpyHostToDevice, s));
+    }
+    return COSPDNN_OK;
+}
+
+}  // namespace
+
 extern "C" int cospdnn_engine_run(cospdnn_engine *e, void *stream) {
     CSP_CHECK(e, COSPDNN_ERR_INVALID, "run: null engine");
     CSP_CHECK(e->built, COSPDNN_ERR_STATE, "run: build first");
     DeviceGuard g(e->device);
+    int rc = take_inputs(e, (cudaStream_t)stream);
+    if (rc) return rc;
     CSP_CUDA(cudaGraphLaunch(e->exec, (cudaStream_t)stream));
     return COSPDNN_OK;
 }
@@ -867,6 +907,8 @@ extern "C" int cospdnn_engine_run_timed(cospdnn_engine *e, void *stream, float *
     CSP_CHECK(e->built, COSPDNN_ERR_STATE, "run_timed: build first");
     DeviceGuard g(e->device);
     cudaStream_t s = (cudaStream_t)stream;
+    int rc = take_inputs(e, s);
+    if (rc) return rc;
     cudaEvent_t a, b;
     CSP_CUDA(cudaEventCreate(&a));
     cudaError_t err = cudaEventCreate(&b);
@@ -973,10 +1015,12 @@ extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, in
     CSP_CHECK(e->built, COSPDNN_ERR_STATE, "profile_layers: build first");
     DeviceGuard g(e->device);
     cudaStream_t s = (cudaStream_t)stream;
+    int rc = take_inputs(e, s);
+    if (rc) return rc;
     cudaEvent_t a, b;
     CSP_CUDA(cudaEventCreate(&a));
     CSP_CUDA(cudaEventCreate(&b));
-    int rc = launch(e->k0, s);
+    rc = launch(e->k0, s);
     int it = 0;
     std::vector<NetState> st(e->nets.size());
     while (!rc && it < max_iters) {

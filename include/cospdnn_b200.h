@@ -162,8 +162,14 @@ int cospdnn_engine_build(cospdnn_engine *e);
 #define COSPDNN_INPUT_U8 0   /* [rows][neuron] bytes (binary images) */
 #define COSPDNN_INPUT_F32 1  /* [rows][neuron] float */
 #define COSPDNN_INPUT_BITS 2 /* [rows][neuron/8] bytes, bit j%8 of byte j/8, LSB first */
-/* Copies Y0 of one network (host pointer: pinned memory keeps it async).
- * Asynchronous on `stream`. */
+/* Copies Y0 of one network (host pointer: pinned memory keeps it async) and
+ * converts it to the compute type.  Asynchronous on `stream`.  Inputs are
+ * double buffered: this fills the network's back buffers and the next run
+ * (cospdnn_engine_run / _run_timed / _profile_layers) makes them current,
+ * so the next batch can be set on another stream while a run is in flight.
+ * The caller orders set_input before the run that should use it (same
+ * stream, or an event), and the second set_input after a run only after
+ * the run before it has finished (the buffers alternate). */
 int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *y0, int format,
                              int on_device, void *stream);
 /* Number of CUDA devices visible to this process (0 when none, or on error);

@@ -285,3 +285,36 @@ def test_engine_edge_cases(cs, prec, kernel):
     for r, (csc, y0, b) in zip(res[1:], nets[1:]):
         check_parity(r, oracle_run(csc, y0, b), len(csc))
     assert res[3]["alive"][1] == 0 and len(res[3]["categories"]) == 0
+
+
+def test_engine_next_input_set_during_run(cs):
+    """Inputs are double buffered: the next batch is copied and converted on
+    a second stream while a run on the first stream still reads the current
+    batch; both runs equal the oracle's."""
+    from netgen import make_random_net
+    n, L = 1024, 6
+    csc, y_a, b = make_random_net(n, L, 800, seed=81)
+    _, y_b, _ = make_random_net(n, 1, 800, seed=82, dlo=0.3, dhi=0.5)
+    ref_a, ref_b = oracle_run(csc, y_a, b), oracle_run(csc, y_b, b)
+    assert not np.array_equal(ref_a["categories"], ref_b["categories"])
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    eng = cs.Engine(0)
+    nid = eng.add_net(n, L, 800, float(b), 1e-5, 1, 0)
+    for l, (cp, ri, vv) in enumerate(csc):
+        eng.set_layer_csc(nid, l, cp, ri, vv)
+    eng.build()
+    got = []
+    for rep in range(2):
+        eng.set_input(nid, torch.from_numpy(np.packbits(y_a, axis=1, bitorder="little")).pin_memory(),
+                      fmt=cs.INPUT_BITS, stream=s1)
+        eng.run(s1)                                   # batch A
+        eng.set_input(nid, y_b, stream=s2)            # batch B, while A runs
+        ev = torch.cuda.Event()
+        ev.record(s2)
+        got.append(eng.result(nid, s1))               # A's result
+        s1.wait_event(ev)
+        eng.run(s1)                                   # batch B
+        got.append(eng.result(nid, s1))
+    eng.close()
+    for r, ref in zip(got, [ref_a, ref_b, ref_a, ref_b]):
+        check_parity(r, ref, L)
