@@ -76,6 +76,139 @@ __global__ void __launch_bounds__(kLayerThreads)
     }
 }
 
+// 16x16 blocks, batch a multiple of 8.  One CTA = 256 batch columns x one
+// block column.  The rows of up to two blocks (32 rows; hi and lo halves, or
+// FP32) are copied into shared memory with cp.async (16-byte pieces,
+// zero-filled past the matrix), so a CTA keeps 32 KB of loads in flight
+// without holding them in registers (about seven CTAs per SM); then each
+// thread sums hi + lo for its 2 columns (exact in FP32: the pair spans at
+// most 22 significant bits) and does 2 FMAs per weight, the block's weights staged transposed ([k][o]) for
+// broadcast 16-byte shared loads.
+constexpr int kFastThreads = 128;
+constexpr int kFastCols = 2;                          // batch columns per thread
+constexpr int kFastChunk = kFastThreads * kFastCols;  // 256 batch columns per CTA
+constexpr int kFastRows = 32;                         // rows staged at once (two blocks)
+constexpr size_t kFastSmem = (size_t)kFastRows * 2 * kFastChunk * 2;  // 32 KB: two 16-bit planes
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pred) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem);
+    const int n = pred ? 16 : 0;  // 0: fill with zeros, read nothing
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "r"(n) : "memory");
+}
+
+template <bool AF32, bool BF32, bool REF_ARITH>
+__global__ void __launch_bounds__(kFastThreads)
+    k_layer_fm16(const void *__restrict__ A, const void *__restrict__ B, float *__restrict__ C,
+                 const int *__restrict__ fuse, const int *__restrict__ idx_ptr, const int *__restrict__ index,
+                 float bias, int batch, int neuron) {
+    extern __shared__ __align__(16) unsigned char fsm[];
+    __shared__ __align__(16) float wT[2][16][16];
+    __shared__ int s_row[kFastRows];
+    // block column fastest in the grid: CTAs running together share batch
+    // columns, so activation rows read by several block columns hit L2
+    const int bid = blockIdx.x;
+    const int c0 = blockIdx.y * kFastChunk;  // first batch column of the CTA
+    const int b0 = threadIdx.x * kFastCols;  // this thread's columns within the chunk
+    float2 acc[16];
+#pragma unroll
+    for (int o = 0; o < 16; ++o) acc[o] = make_float2(0.f, 0.f);
+    const int p0 = idx_ptr[bid];
+    const int p1 = REF_ARITH ? p0 + 2 : idx_ptr[bid + 1];
+    // 16-bit input: plane 0 = hi rows, plane 1 = lo rows, each [32][512] halves;
+    // FP32 input: one [32][512] float plane in the same bytes
+    __half *hs = reinterpret_cast<__half *>(fsm);
+    float *fs = reinterpret_cast<float *>(fsm);
+    for (int q0 = p0; q0 < p1; q0 += 2) {
+        const int nb = min(2, p1 - q0);
+        __syncthreads();  // the previous stage's rows and weights are consumed
+        if (threadIdx.x < kFastRows) {
+            const int t = threadIdx.x, r = t < nb * 16 ? index[q0 + (t >> 4)] + (t & 15) : -1;
+            int f = -1;
+            if (r >= 0 && r < neuron) f = fuse ? fuse[r] : r;
+            s_row[t] = (f >= 0 && f < neuron) ? f : -1;
+        }
+        for (int t = threadIdx.x; t < nb * 256; t += kFastThreads) {
+            const int j = t >> 8, k = (t >> 4) & 15, o = t & 15;
+            // REF_ARITH: value [k*16 + o] feeds output o from input start+k;
+            // otherwise value [o*16 + k] is W[start+k][col_start+o]
+            const int64_t g = (int64_t)(q0 + j) * 256 + (REF_ARITH ? k * 16 + o : o * 16 + k);
+            wT[j][k][o] = BF32 ? ((const float *)B)[g] : __half2float(((const __half *)B)[g]);
+        }
+        __syncthreads();
+        // asynchronous copies: 16-byte pieces of every staged row
+        constexpr int kPiecesPerRow = AF32 ? kFastChunk * 4 / 16 : kFastChunk * 2 / 16;
+        constexpr int kPlanes = AF32 ? 1 : 2;
+        const int total = nb * 16 * kPiecesPerRow * kPlanes;
+        for (int i = threadIdx.x; i < total; i += kFastThreads) {
+            const int pc = i % kPiecesPerRow, rowp = i / kPiecesPerRow;
+            const int t = rowp % (nb * 16), plane = rowp / (nb * 16);
+            const int f = s_row[t];
+            const int col = c0 + pc * (AF32 ? 4 : 8);
+            const bool ok = f >= 0 && col < batch;
+            if (AF32) {
+                const float *src = ok ? (const float *)A + (int64_t)f * batch + col : (const float *)A;
+                cp_async16(fs + (int64_t)t * kFastChunk + pc * 4, src, ok);
+            } else {
+                const __half *src = ok ? (const __half *)A + (int64_t)(f + plane * neuron) * batch + col
+                                       : (const __half *)A;
+                cp_async16(hs + ((int64_t)plane * kFastRows + t) * kFastChunk + pc * 8, src, ok);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        for (int t = 0; t < nb * 16; ++t) {
+            float2 a;
+            if (AF32) {
+                a = *reinterpret_cast<const float2 *>(fs + (int64_t)t * kFastChunk + b0);
+            } else {
+                const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(hs + (int64_t)t * kFastChunk + b0));
+                const float2 l = __half22float2(
+                    *reinterpret_cast<const __half2 *>(hs + (int64_t)(kFastRows + t) * kFastChunk + b0));
+                a = make_float2(h.x + l.x, h.y + l.y);
+            }
+            const int j = t >> 4, k = t & 15;
+#pragma unroll
+            for (int o4 = 0; o4 < 16; o4 += 4) {
+                const float4 w = *reinterpret_cast<const float4 *>(&wT[j][k][o4]);
+                const float ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    acc[o4 + q].x = fmaf(ws[q], a.x, acc[o4 + q].x);
+                    acc[o4 + q].y = fmaf(ws[q], a.y, acc[o4 + q].y);
+                }
+            }
+        }
+    }
+    const int col = c0 + b0;
+    if (col >= batch) return;  // batch % 8 == 0: the thread's two columns both exist
+#pragma unroll
+    for (int o = 0; o < 16; ++o) {
+        const int out = bid * 16 + o;
+        if (out < neuron)
+            *reinterpret_cast<float2 *>(C + (int64_t)out * batch + col) =
+                make_float2(clamp32(acc[o].x + bias), clamp32(acc[o].y + bias));
+    }
+}
+
+void launch_layer_fast(dim3 grid, cudaStream_t s, unsigned flags, const void *A, const void *B, float *C,
+                       const int *fuse, const int *idx_ptr, const int *index, float bias, int batch, int neuron) {
+    const bool af = flags & COSPDNN_LAYER_A_FLOAT, bf = flags & COSPDNN_LAYER_B_FLOAT;
+    const bool ra = flags & COSPDNN_LAYER_REFERENCE_ARITH;
+#define CSP_F(AF, BF, RA)                                                                                     \
+    do {                                                                                                      \
+        cudaFuncSetAttribute(k_layer_fm16<AF, BF, RA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFastSmem); \
+        k_layer_fm16<AF, BF, RA><<<grid, kFastThreads, kFastSmem, s>>>(A, B, C, fuse, idx_ptr, index, bias, batch, neuron); \
+    } while (0)
+    if (af) {
+        if (bf) { if (ra) CSP_F(true, true, true); else CSP_F(true, true, false); }
+        else { if (ra) CSP_F(true, false, true); else CSP_F(true, false, false); }
+    } else {
+        if (bf) { if (ra) CSP_F(false, true, true); else CSP_F(false, true, false); }
+        else { if (ra) CSP_F(false, false, true); else CSP_F(false, false, false); }
+    }
+#undef CSP_F
+}
+
 template <int BC>
 void launch_layer(dim3 grid, cudaStream_t s, unsigned flags, const void *A, const void *B,
                   float *C, const int *fuse, const int *idx_ptr, const int *index, float bias,
@@ -214,8 +347,17 @@ extern "C" int cospdnn_layer(const void *A, const void *B, float *C, const int *
     if (flags & COSPDNN_LAYER_REFERENCE_ARITH)
         CSP_CHECK(blocksize_c == 16 && blocksize_r == 16, COSPDNN_ERR_UNSUPPORTED,
                   "cospdnn_layer: reference arithmetic needs 16x16 blocks");
-    const dim3 grid((batch + kLayerThreads - 1) / kLayerThreads, nblockcols);
     cudaStream_t s = (cudaStream_t)stream;
+    const bool aligned = ((uintptr_t)A % 16 == 0) && ((uintptr_t)C % 16 == 0);
+    if (blocksize_c == 16 && blocksize_r == 16 && batch % 8 == 0 && aligned) {
+        const int per = kFastChunk;
+        CSP_CHECK((batch + per - 1) / per <= 65535, COSPDNN_ERR_UNSUPPORTED, "cospdnn_layer: batch too large");
+        launch_layer_fast(dim3(nblockcols, (batch + per - 1) / per), s, flags, A, B, C, fuse, idx_ptr, index, bias,
+                          batch, neuron);
+        CSP_CUDA(cudaGetLastError());
+        return COSPDNN_OK;
+    }
+    const dim3 grid((batch + kLayerThreads - 1) / kLayerThreads, nblockcols);
     switch (blocksize_c) {
         case 8: launch_layer<8>(grid, s, flags, A, B, C, fuse, idx_ptr, index, bias, batch, neuron, blocksize_r); break;
         case 16: launch_layer<16>(grid, s, flags, A, B, C, fuse, idx_ptr, index, bias, batch, neuron, blocksize_r); break;

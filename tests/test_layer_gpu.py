@@ -43,7 +43,7 @@ def dev(x, dt=None):
     return t.cuda()
 
 
-@pytest.mark.parametrize("batch", [128, 300])
+@pytest.mark.parametrize("batch", [128, 300, 301])  # 301: not a multiple of 4, the general kernel
 @pytest.mark.parametrize("kind", ["xor", "r1"])
 def test_layer_true_product(cs, oracle, batch, kind):
     n = 256

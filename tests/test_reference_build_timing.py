@@ -59,3 +59,64 @@ def test_reference_build_timing(oracle, name, neuron, kind):
     if out:
         with open(out, "a") as f:
             f.write(json.dumps(line) + "\n")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference not built (make -C oracle ref)")
+@pytest.mark.parametrize("neuron", [1024, 4096])
+def test_layer_entry_timing_vs_reference_kernel(oracle, neuron):
+    """The drop-in layer entry beside the reference's cospdnn_single on the
+    same buffers: its BCSC of one R1 layer (two dense blocks per column, what
+    its kernel computes in full), hi/lo FP16 activations of 60032 columns.
+    CUDA-event time per launch (median of 20, after 5 warm-up launches); the
+    outputs agree in the reference-arithmetic mode where the reference's
+    last-stage race cannot act (weights only in one quadrant of each block)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import cospdnn_b200 as cs
+    from test_layer_gpu import _ref_kernel, dev, hilo
+    from cospdnn_b200 import synth
+    batch = 60032  # 60000 padded to the reference kernel's 64-column tile, as its host loop does (src/cospdnn.cu:24)
+    cp, ri, vv = synth.network(neuron, 1, SEED, net=0, kind="r1")[0]
+    row, col, val = oracle.csc_to_coo(cp, ri, vv)
+    bcp, bri, _, bvals = oracle.bcsc_greedy(row, col, val, 16)
+    V = bvals.reshape(-1, 16, 16)
+    V[:, 8:, :] = 0  # race-free (as in the reference pin of test_layer_gpu.py):
+    V[:, :, 8:] = 0  # only the [k<8][r<8] quadrant of each block is non-zero
+    bvals = np.ascontiguousarray(V.reshape(-1))
+    rng = np.random.default_rng(5)
+    a = (rng.random((neuron, batch)) < 0.2).astype(np.float32)
+    A, B = dev(hilo(a)), dev(bvals, torch.float16)
+    F = dev(np.arange(neuron, dtype=np.int32))
+    P, I = dev(bcp), dev(bri)
+    nbc = len(bcp) - 1
+    ref = _ref_kernel()
+    out_ref = torch.empty((neuron, batch), dtype=torch.float32, device="cuda")
+    out = torch.empty_like(out_ref)
+
+    def time_it(fn):
+        for _ in range(5):
+            fn()
+        ts = []
+        for _ in range(20):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    t_ref = time_it(lambda: ref.ref_cospdnn_single(A.data_ptr(), B.data_ptr(), out_ref.data_ptr(), F.data_ptr(),
+                                                   P.data_ptr(), I.data_ptr(), -0.35, batch, neuron, nbc, None))
+    t_ra = time_it(lambda: cs.layer(A, B, out, F, P, I, -0.35, batch, neuron, flags=cs.LAYER_REFERENCE_ARITH))
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(out.cpu().numpy(), out_ref.cpu().numpy(), rtol=0, atol=5e-5)
+    t_true = time_it(lambda: cs.layer(A, B, out, F, P, I, -0.35, batch, neuron))
+    line = {"workload": f"one R1 layer, {neuron} neurons, batch {batch}, hi/lo FP16 activations",
+            "reference_cospdnn_single_ms": t_ref, "cospdnn_layer_reference_arith_ms": t_ra,
+            "cospdnn_layer_true_product_ms": t_true}
+    print(json.dumps(line))
+    out_path = os.environ.get("COSPDNN_REF_TIMING_OUT")
+    if out_path:
+        with open(out_path, "a") as f:
+            f.write(json.dumps(line) + "\n")
