@@ -97,6 +97,19 @@ __device__ __forceinline__ void fma2(float &a0, float &a1, uint32_t ent, uint32_
         : "r"(ent), "r"(y));
 }
 
+// a0 += w * y0, a1 += w * y1 in one sm_100 packed instruction (fma.rn.f32x2:
+// two IEEE FMAs, bit-identical to fmaf on each lane).
+__device__ __forceinline__ void ffma2(float &a0, float &a1, float w, uint32_t y0, uint32_t y1) {
+    asm("{\n\t.reg .b64 d, x, w;\n\t"
+        "mov.b64 d, {%0, %1};\n\t"
+        "mov.b64 x, {%2, %3};\n\t"
+        "mov.b64 w, {%4, %4};\n\t"
+        "fma.rn.f32x2 d, w, x, d;\n\t"
+        "mov.b64 {%0, %1}, d;\n\t}"
+        : "+f"(a0), "+f"(a1)
+        : "r"(y0), "r"(y1), "f"(w));
+}
+
 // V = LB / elem FMAs of one entry on one LB-byte shared load (V rows of one
 // input).
 template <typename T, int LB>
@@ -104,9 +117,7 @@ __device__ __forceinline__ void cc_entry(float *acc, uint32_t w, uint32_t addr) 
     if constexpr (LB == 8) {
         const uint2 y = lds64(addr);
         if constexpr (sizeof(T) == 4) {
-            const float wf = __uint_as_float(w);
-            acc[0] = fmaf(wf, __uint_as_float(y.x), acc[0]);
-            acc[1] = fmaf(wf, __uint_as_float(y.y), acc[1]);
+            ffma2(acc[0], acc[1], __uint_as_float(w), y.x, y.y);
         } else {
             fma2(acc[0], acc[1], w, y.x, T());
             fma2(acc[2], acc[3], w, y.y, T());
@@ -116,10 +127,8 @@ __device__ __forceinline__ void cc_entry(float *acc, uint32_t w, uint32_t addr) 
     const uint4 y = lds128(addr);
     if constexpr (sizeof(T) == 4) {
         const float wf = __uint_as_float(w);
-        acc[0] = fmaf(wf, __uint_as_float(y.x), acc[0]);
-        acc[1] = fmaf(wf, __uint_as_float(y.y), acc[1]);
-        acc[2] = fmaf(wf, __uint_as_float(y.z), acc[2]);
-        acc[3] = fmaf(wf, __uint_as_float(y.w), acc[3]);
+        ffma2(acc[0], acc[1], wf, y.x, y.y);
+        ffma2(acc[2], acc[3], wf, y.z, y.w);
     } else {
         fma2(acc[0], acc[1], w, y.x, T());
         fma2(acc[2], acc[3], w, y.y, T());
