@@ -76,26 +76,22 @@ __global__ void __launch_bounds__(kLayerThreads)
     }
 }
 
-// 16x16 blocks, batch a multiple of 8.  CTA (x, y) computes block column x
-// for batch chunks y, y + gridDim.y, ... of 256 columns (one chunk per CTA
-// up to 65535 chunks).  Per chunk the column's blocks go in stages of two:
-// the stage's 32 input rows (through `fuse`) and its weights, transposed to
-// [k][o] for broadcast 16-byte shared loads, are loaded; each block's rows
-// for the chunk (hi and lo planes, or FP32) are copied into shared memory
-// with cp.async as one copy group (16-byte pieces, zero-filled past the
-// matrix or for a dropped row), so the second block lands while the first
-// is computed and a CTA keeps 32 KB of loads in flight without holding them
-// in registers (six CTAs per SM).  Each thread sums hi + lo for its 2
-// columns (exact in FP32: the pair spans at most 22 significant bits) and
-// does one packed two-lane FMA per weight (fma.rn.f32x2: two IEEE FMAs,
-// identical to fmaf on each column).
+// 16x16 blocks, batch a multiple of 8.  One CTA = 256 batch columns x one
+// block column.  The rows of up to two blocks (32 rows; hi and lo halves, or
+// FP32) are copied into shared memory with cp.async (16-byte pieces,
+// zero-filled past the matrix), one copy group per block so the second block
+// lands while the first is computed; a CTA keeps 32 KB of loads in flight
+// without holding them in registers (six CTAs per SM).  Each thread sums
+// hi + lo for its 2 columns (exact in FP32: the pair spans at most 22
+// significant bits) and does one packed two-lane FMA per weight
+// (fma.rn.f32x2: two IEEE FMAs, identical to fmaf on each column), the
+// block's weights staged transposed ([k][o]) for broadcast 16-byte shared
+// loads.
 constexpr int kFastThreads = 128;
 constexpr int kFastCols = 2;                          // batch columns per thread
-constexpr int kFastChunk = kFastThreads * kFastCols;  // 256 batch columns per chunk
-constexpr int kFastCtasPerSm = 6;                     // resident CTAs the registers must allow
-constexpr int kStageBytes = 16 * 2 * kFastChunk * 2;  // 16 KB: one block's 16 rows, two 16-bit planes (or FP32)
-constexpr size_t kMetaBytes = 2 * 16 * 16 * 4 + 32 * 4;
-constexpr size_t kFastSmem = 2 * (size_t)kStageBytes + kMetaBytes;  // 34.1 KB
+constexpr int kFastChunk = kFastThreads * kFastCols;  // 256 batch columns per CTA
+constexpr int kFastRows = 32;                         // rows staged at once (two blocks)
+constexpr size_t kFastSmem = (size_t)kFastRows * 2 * kFastChunk * 2;  // 32 KB: two 16-bit planes
 
 // acc.x += w * a.x, acc.y += w * a.y in one sm_100 packed instruction
 __device__ __forceinline__ void ffma2(float2 &acc, float w, float2 a) {
@@ -115,77 +111,97 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool pr
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gmem), "r"(n) : "memory");
 }
 
-// Input row of block slot t's local row r (fused, range-checked), -1 when
-// the row is dropped.
-__device__ __forceinline__ int fm16_row(const int *__restrict__ fuse, const int *__restrict__ index, int q, int r,
-                                        int neuron) {
-    const int g = index[q] + r;
-    int f = -1;
-    if (g >= 0 && g < neuron) f = fuse ? fuse[g] : g;
-    return (f >= 0 && f < neuron) ? f : -1;
-}
-
-// Weight (k, o) of block q: REF_ARITH value [k*16 + o] feeds output o from
-// input start+k (the reference's ldmatrix.trans pairing); otherwise value
-// [o*16 + k] is W[start+k][col_start+o].
-template <bool BF32, bool REF_ARITH>
-__device__ __forceinline__ float fm16_weight(const void *__restrict__ B, int q, int k, int o) {
-    const int64_t g = (int64_t)q * 256 + (REF_ARITH ? k * 16 + o : o * 16 + k);
-    return BF32 ? ((const float *)B)[g] : __half2float(((const __half *)B)[g]);
-}
-
-// Copies block slot `rows` (16 row ids) for the chunk at column c0 into the
-// 16 KB slot `dst`: 1024 16-byte pieces, 8 per thread.
-template <bool AF32>
-__device__ __forceinline__ void fm16_issue(const void *__restrict__ A, const int *rows, unsigned char *dst, int c0,
-                                           int batch, int neuron) {
-    constexpr int kPiecesPerRow = AF32 ? kFastChunk * 4 / 16 : kFastChunk * 2 / 16;
-#pragma unroll 2
-    for (int u = 0; u < 8; ++u) {  // 8 * kFastThreads pieces per stage
-        const int i = threadIdx.x + u * kFastThreads;
-        const int pc = i % kPiecesPerRow, rowp = i / kPiecesPerRow;
-        const int r = rowp & 15, plane = rowp >> 4;  // plane 0 only for FP32
-        const int f = rows[r];
-        const int col = c0 + pc * (AF32 ? 4 : 8);
-        const bool ok = f >= 0 && col < batch;
-        if (AF32) {
-            const float *src = ok ? (const float *)A + (int64_t)f * batch + col : (const float *)A;
-            cp_async16(reinterpret_cast<float *>(dst) + r * kFastChunk + pc * 4, src, ok);
-        } else {
-            const __half *src = ok ? (const __half *)A + (int64_t)(f + plane * neuron) * batch + col
-                                   : (const __half *)A;
-            cp_async16(reinterpret_cast<__half *>(dst) + (plane * 16 + r) * kFastChunk + pc * 8, src, ok);
-        }
-    }
-}
-
-// acc += the block staged in `src` (16 rows) times its weights wT[k][o].
-template <bool AF32>
-__device__ __forceinline__ void fm16_compute(float2 *acc, const unsigned char *src, const float *wT, int b0) {
-#pragma unroll 4
-    for (int k = 0; k < 16; ++k) {
-        float2 a;
-        if (AF32) {
-            a = *reinterpret_cast<const float2 *>(reinterpret_cast<const float *>(src) + k * kFastChunk + b0);
-        } else {
-            const __half *hs = reinterpret_cast<const __half *>(src);
-            const float2 h = __half22float2(*reinterpret_cast<const __half2 *>(hs + k * kFastChunk + b0));
-            const float2 l = __half22float2(*reinterpret_cast<const __half2 *>(hs + (16 + k) * kFastChunk + b0));
-            a = make_float2(h.x + l.x, h.y + l.y);
-        }
+template <bool AF32, bool BF32, bool REF_ARITH>
+__global__ void __launch_bounds__(kFastThreads)
+    k_layer_fm16(const void *__restrict__ A, const void *__restrict__ B, float *__restrict__ C,
+                 const int *__restrict__ fuse, const int *__restrict__ idx_ptr, const int *__restrict__ index,
+                 float bias, int batch, int neuron) {
+    extern __shared__ __align__(16) unsigned char fsm[];
+    __shared__ __align__(16) float wT[2][16][16];
+    __shared__ int s_row[kFastRows];
+    // block column fastest in the grid: CTAs running together share batch
+    // columns, so activation rows read by several block columns hit L2
+    const int bid = blockIdx.x;
+    const int c0 = blockIdx.y * kFastChunk;  // first batch column of the CTA
+    const int b0 = threadIdx.x * kFastCols;  // this thread's columns within the chunk
+    float2 acc[16];
 #pragma unroll
-        for (int o4 = 0; o4 < 16; o4 += 4) {
-            const float4 w = *reinterpret_cast<const float4 *>(wT + k * 16 + o4);
-            ffma2(acc[o4], w.x, a);
-            ffma2(acc[o4 + 1], w.y, a);
-            ffma2(acc[o4 + 2], w.z, a);
-            ffma2(acc[o4 + 3], w.w, a);
+    for (int o = 0; o < 16; ++o) acc[o] = make_float2(0.f, 0.f);
+    const int p0 = idx_ptr[bid];
+    const int p1 = REF_ARITH ? p0 + 2 : idx_ptr[bid + 1];
+    // 16-bit input: plane 0 = hi rows, plane 1 = lo rows, each [32][512] halves;
+    // FP32 input: one [32][512] float plane in the same bytes
+    __half *hs = reinterpret_cast<__half *>(fsm);
+    float *fs = reinterpret_cast<float *>(fsm);
+    for (int q0 = p0; q0 < p1; q0 += 2) {
+        const int nb = min(2, p1 - q0);
+        __syncthreads();  // the previous stage's rows and weights are consumed
+        if (threadIdx.x < kFastRows) {
+            const int t = threadIdx.x, r = t < nb * 16 ? index[q0 + (t >> 4)] + (t & 15) : -1;
+            int f = -1;
+            if (r >= 0 && r < neuron) f = fuse ? fuse[r] : r;
+            s_row[t] = (f >= 0 && f < neuron) ? f : -1;
+        }
+        for (int t = threadIdx.x; t < nb * 256; t += kFastThreads) {
+            const int j = t >> 8, k = (t >> 4) & 15, o = t & 15;
+            // REF_ARITH: value [k*16 + o] feeds output o from input start+k;
+            // otherwise value [o*16 + k] is W[start+k][col_start+o]
+            const int64_t g = (int64_t)(q0 + j) * 256 + (REF_ARITH ? k * 16 + o : o * 16 + k);
+            wT[j][k][o] = BF32 ? ((const float *)B)[g] : __half2float(((const __half *)B)[g]);
+        }
+        __syncthreads();
+        constexpr int kPiecesPerRow = AF32 ? kFastChunk * 4 / 16 : kFastChunk * 2 / 16;
+        constexpr int kPlanes = AF32 ? 1 : 2;
+        constexpr int kPerBlock = 16 * kPiecesPerRow * kPlanes;
+        for (int j = 0; j < nb; ++j) {
+            for (int i = threadIdx.x; i < kPerBlock; i += kFastThreads) {
+                const int pc = i % kPiecesPerRow, rowp = i / kPiecesPerRow;
+                const int t = j * 16 + (rowp & 15), plane = rowp >> 4;
+                const int f = s_row[t];
+                const int col = c0 + pc * (AF32 ? 4 : 8);
+                const bool ok = f >= 0 && col < batch;
+                if (AF32) {
+                    const float *src = ok ? (const float *)A + (int64_t)f * batch + col : (const float *)A;
+                    cp_async16(fs + (int64_t)t * kFastChunk + pc * 4, src, ok);
+                } else {
+                    const __half *src = ok ? (const __half *)A + (int64_t)(f + plane * neuron) * batch + col
+                                           : (const __half *)A;
+                    cp_async16(hs + ((int64_t)plane * kFastRows + t) * kFastChunk + pc * 8, src, ok);
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        for (int j = 0; j < nb; ++j) {
+            if (j + 1 < nb)
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            else
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncthreads();
+#pragma unroll 4
+            for (int k = 0; k < 16; ++k) {
+                const int t = j * 16 + k;
+                float2 a;
+                if (AF32) {
+                    a = *reinterpret_cast<const float2 *>(fs + (int64_t)t * kFastChunk + b0);
+                } else {
+                    const float2 h =
+                        __half22float2(*reinterpret_cast<const __half2 *>(hs + (int64_t)t * kFastChunk + b0));
+                    const float2 l = __half22float2(
+                        *reinterpret_cast<const __half2 *>(hs + (int64_t)(kFastRows + t) * kFastChunk + b0));
+                    a = make_float2(h.x + l.x, h.y + l.y);
+                }
+#pragma unroll
+                for (int o4 = 0; o4 < 16; o4 += 4) {
+                    const float4 w = *reinterpret_cast<const float4 *>(&wT[j][k][o4]);
+                    ffma2(acc[o4], w.x, a);
+                    ffma2(acc[o4 + 1], w.y, a);
+                    ffma2(acc[o4 + 2], w.z, a);
+                    ffma2(acc[o4 + 3], w.w, a);
+                }
+            }
         }
     }
-}
-
-__device__ __forceinline__ void fm16_store(const float2 *acc, float *__restrict__ C, float bias, int bid, int col,
-                                           int batch, int neuron) {
+    const int col = c0 + b0;
     if (col >= batch) return;  // batch % 8 == 0: the thread's two columns both exist
 #pragma unroll
     for (int o = 0; o < 16; ++o) {
@@ -194,65 +210,6 @@ __device__ __forceinline__ void fm16_store(const float2 *acc, float *__restrict_
             *reinterpret_cast<float2 *>(C + (int64_t)out * batch + col) =
                 make_float2(clamp32(acc[o].x + bias), clamp32(acc[o].y + bias));
     }
-}
-
-// One chunk of a block column: stages of two blocks (two copy groups, the
-// second landing while the first is computed), metadata loaded per stage.
-template <bool AF32, bool BF32, bool REF_ARITH>
-__device__ __forceinline__ void fm16_chunk(const void *__restrict__ A, const void *__restrict__ B, float *__restrict__ C,
-                           const int *__restrict__ fuse, int p0, int p1, const int *__restrict__ index,
-                           float bias, int batch, int neuron, int bid, int c0, unsigned char *ring, float *wT,
-                           int *s_row) {
-    const int b0 = threadIdx.x * kFastCols;
-    float2 acc[16];
-#pragma unroll
-    for (int o = 0; o < 16; ++o) acc[o] = make_float2(0.f, 0.f);
-    for (int q0 = p0; q0 < p1; q0 += 2) {
-        const int nb = min(2, p1 - q0);
-        __syncthreads();  // the previous stage's rows and weights are consumed
-        if (threadIdx.x < 32) s_row[threadIdx.x] = threadIdx.x < nb * 16
-                                                        ? fm16_row(fuse, index, q0 + (threadIdx.x >> 4), threadIdx.x & 15, neuron)
-                                                        : -1;
-        for (int t = threadIdx.x; t < nb * 256; t += kFastThreads)
-            wT[t] = fm16_weight<BF32, REF_ARITH>(B, q0 + (t >> 8), (t >> 4) & 15, t & 15);
-        __syncthreads();
-        for (int j = 0; j < nb; ++j) {
-            fm16_issue<AF32>(A, s_row + 16 * j, ring + j * kStageBytes, c0, batch, neuron);
-            asm volatile("cp.async.commit_group;" ::: "memory");
-        }
-        for (int j = 0; j < nb; ++j) {
-            if (j + 1 < nb)
-                asm volatile("cp.async.wait_group 1;" ::: "memory");
-            else
-                asm volatile("cp.async.wait_group 0;" ::: "memory");
-            __syncthreads();  // every thread's pieces of block j have landed
-            fm16_compute<AF32>(acc, ring + j * kStageBytes, wT + 256 * j, b0);
-        }
-    }
-    fm16_store(acc, C, bias, bid, c0 + b0, batch, neuron);
-}
-
-template <bool AF32, bool BF32, bool REF_ARITH>
-__global__ void __launch_bounds__(kFastThreads, kFastCtasPerSm)
-    k_layer_fm16(const void *__restrict__ A, const void *__restrict__ B, float *__restrict__ C,
-                 const int *__restrict__ fuse, const int *__restrict__ idx_ptr, const int *__restrict__ index,
-                 float bias, int batch, int neuron) {
-    extern __shared__ __align__(16) unsigned char fsm[];
-    unsigned char *ring = fsm;
-    float *wT = reinterpret_cast<float *>(fsm + 2 * (size_t)kStageBytes);  // [block][k][o]
-    int *s_row = reinterpret_cast<int *>(wT + 2 * 256);                    // [block][r]
-    const int bid = blockIdx.x;
-    const int nchunks = (batch + kFastChunk - 1) / kFastChunk;
-    const int p0 = idx_ptr[bid];
-    const int p1 = REF_ARITH ? p0 + 2 : idx_ptr[bid + 1];
-    for (int y = blockIdx.y; y < nchunks; y += gridDim.y)
-        fm16_chunk<AF32, BF32, REF_ARITH>(A, B, C, fuse, p0, p1, index, bias, batch, neuron, bid, y * kFastChunk,
-                                          ring, wT, s_row);
-}
-
-dim3 fast_grid(int nblockcols, int batch) {
-    const int nchunks = (batch + kFastChunk - 1) / kFastChunk;
-    return dim3(nblockcols, std::min(nchunks, 65535));
 }
 
 void launch_layer_fast(dim3 grid, cudaStream_t s, unsigned flags, const void *A, const void *B, float *C,
@@ -415,8 +372,10 @@ extern "C" int cospdnn_layer(const void *A, const void *B, float *C, const int *
     cudaStream_t s = (cudaStream_t)stream;
     const bool aligned = ((uintptr_t)A % 16 == 0) && ((uintptr_t)C % 16 == 0);
     if (blocksize_c == 16 && blocksize_r == 16 && batch % 8 == 0 && aligned) {
-        launch_layer_fast(fast_grid(nblockcols, batch), s, flags, A, B, C, fuse, idx_ptr, index, bias, batch,
-                          neuron);
+        const int per = kFastChunk;
+        CSP_CHECK((batch + per - 1) / per <= 65535, COSPDNN_ERR_UNSUPPORTED, "cospdnn_layer: batch too large");
+        launch_layer_fast(dim3(nblockcols, (batch + per - 1) / per), s, flags, A, B, C, fuse, idx_ptr, index, bias,
+                          batch, neuron);
         CSP_CUDA(cudaGetLastError());
         return COSPDNN_OK;
     }
