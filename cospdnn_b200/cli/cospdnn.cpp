@@ -6,7 +6,10 @@
 // "layer l, feature = n" (rows alive after layer l) and
 // "Kernel Exec Time = X ms".  With gpu_num > 1 the batch is split into
 // contiguous row ranges, one engine and host thread per GPU, and the counts
-// are summed.  COSPDNN_PRECISION / COSPDNN_KERNEL select precision and kernel.
+// are summed.  COSPDNN_PRECISION / COSPDNN_KERNEL select precision and kernel;
+// COSPDNN_CACHE keeps parsed datasets in binary form; COSPDNN_CATEGORIES /
+// COSPDNN_TRUTH write the categories in Graph Challenge format and check them
+// against a truth file (exit status 2 on a mismatch).  See reference_io.h.
 #include <algorithm>
 #include <thread>
 
@@ -45,6 +48,7 @@ int main(int argc, char *argv[]) {
     const int ng = (int)devices.size();
     std::vector<std::vector<int64_t>> alive(ng, std::vector<int64_t>(layers, 0));
     std::vector<int64_t> count(ng, 0);
+    std::vector<std::vector<int32_t>> cats(ng);
     std::vector<float> ms(ng, 0.0f);
     // each worker exits the process with the reference's style of message on
     // any error (as Safe_Call does in the reference)
@@ -56,7 +60,10 @@ int main(int argc, char *argv[]) {
         check(cospdnn_engine_build(e), "build");
         set_rows(e, id, net, r0, r1);
         check(cospdnn_engine_run_timed(e, nullptr, &ms[g]), "run");
-        check(cospdnn_engine_result(e, id, nullptr, &count[g], alive[g].data(), nullptr, nullptr), "result");
+        cats[g].assign((size_t)std::max(1, r1 - r0), 0);
+        check(cospdnn_engine_result(e, id, cats[g].data(), &count[g], alive[g].data(), nullptr, nullptr), "result");
+        cats[g].resize((size_t)count[g]);
+        for (auto &c : cats[g]) c += r0;  // rows of the whole batch
         cospdnn_engine_destroy(e);
     };
     if (ng == 1) {
@@ -79,7 +86,10 @@ int main(int argc, char *argv[]) {
         tmax = std::max(tmax, ms[g]);
     }
     std::cout << "[Categories] :" << total << std::endl;
+    std::vector<int64_t> all;
+    for (int g = 0; g < ng; ++g) all.insert(all.end(), cats[g].begin(), cats[g].end());
+    const int rc = report_categories(all, "COSPDNN_CATEGORIES", "COSPDNN_TRUTH", "");
     std::cout << "Kernel Exec Time = " << tmax << "ms" << std::endl;
     std::cout << "[END]..." << std::endl;
-    return 0;
+    return rc;
 }

@@ -5,7 +5,8 @@
 // may differ in width, depth and batch).  Prints the reference's lines
 // "SpDNN 1 layer l, feature = n", "SpDNN 2 layer l, feature = n" and
 // "Total Kernel Exec Time = X ms".  COSPDNN_PRECISION / COSPDNN_KERNEL select
-// precision and kernel.
+// precision and kernel; COSPDNN_CACHE, COSPDNN_CATEGORIES_1/_2 and
+// COSPDNN_TRUTH_1/_2 as in cospdnn.out (exit status 2 on a mismatch).
 #include "reference_io.h"
 
 using namespace cospdnn_cli;
@@ -41,16 +42,22 @@ int main(int argc, char *argv[]) {
     for (int i = 0; i < 2; ++i) set_rows(e, id[i], net[i], 0, batch[i]);
     float ms = 0.0f;
     check(cospdnn_engine_run_timed(e, nullptr, &ms), "run");
+    int rc = 0;
     for (int i = 0; i < 2; ++i) {
         std::vector<int64_t> alive(layers[i], 0);
+        std::vector<int32_t> cats((size_t)batch[i], 0);
         int64_t count = 0;
-        check(cospdnn_engine_result(e, id[i], nullptr, &count, alive.data(), nullptr, nullptr), "result");
+        check(cospdnn_engine_result(e, id[i], cats.data(), &count, alive.data(), nullptr, nullptr), "result");
         for (int l = 0; l < layers[i]; ++l)
             std::cout << "SpDNN " << i + 1 << " layer " << l << ", feature = " << alive[l] << std::endl;
         std::cout << "[Categories" << i + 1 << "] :" << count << std::endl;
+        const std::vector<int64_t> c64(cats.begin(), cats.begin() + count);
+        const std::string k = std::to_string(i + 1);
+        rc = std::max(rc, report_categories(c64, ("COSPDNN_CATEGORIES_" + k).c_str(), ("COSPDNN_TRUTH_" + k).c_str(),
+                                            "SpDNN " + k + " "));
     }
     cospdnn_engine_destroy(e);
     std::cout << "Total Kernel Exec Time = " << ms << "ms" << std::endl;
     std::cout << "[END]..." << std::endl;
-    return 0;
+    return rc;
 }

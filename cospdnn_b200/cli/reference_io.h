@@ -14,14 +14,31 @@
 // The reference multiplies the value of weight (u, v) with activation row
 // fuse[l][u] (src/kernels/kernel.cu:257-275); the layer handed to the engine
 // is therefore W[fuse[l][u]][v] += val, the true product over every weight.
+//
+// Binary cache (COSPDNN_CACHE=<dir>): a parsed network is kept in
+// <dir>/cospdnn-n{N}-b{B}-l{L}.bin -- the input rows (bytes when integral)
+// and every layer's CSC with the fuse applied -- behind a header holding the
+// size and modification time of every source file; a run whose sources no
+// longer match the header parses the TSV files again and rewrites the cache
+// (written to a temporary name, then renamed).
+//
+// Categories (Graph Challenge format): the surviving input rows, 1-based,
+// one per line, ascending.  COSPDNN_CATEGORIES=<file> writes them and
+// COSPDNN_TRUTH=<file> compares them with a truth file of that format
+// (cospdnn_double.out: COSPDNN_CATEGORIES_1/_2, COSPDNN_TRUTH_1/_2).
 #pragma once
+
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <iostream>
+#include <iterator>
 #include <string>
 #include <utility>
 #include <vector>
@@ -136,7 +153,19 @@ struct Network {
     std::vector<Csc> w;
 };
 
-inline Network load_network(int neuron, int batch, int layers, const std::string &dir) {
+inline std::string input_path(int neuron, const std::string &dir) {
+    return dir + "/sparse-images-" + std::to_string(neuron) + ".tsv";
+}
+inline std::string fuse_path(int neuron, int layers, const std::string &dir) {
+    return dir + "/fuse_matrix/neuron" + std::to_string(neuron) + "/" + std::to_string(neuron) + "_" +
+           std::to_string(layers) + "_fuse.tsv";
+}
+inline std::string layer_path(int neuron, int l, const std::string &dir) {
+    return dir + "/neuron" + std::to_string(neuron) + "/" + std::to_string(neuron) + "-l" + std::to_string(l + 1) +
+           ".tsv";
+}
+
+inline Network parse_network(int neuron, int batch, int layers, const std::string &dir) {
     Network n;
     n.neuron = neuron;
     n.batch = batch;
@@ -145,6 +174,197 @@ inline Network load_network(int neuron, int batch, int layers, const std::string
     const auto fuse = read_fuse(neuron, layers, dir);
     for (int l = 0; l < layers; ++l) n.w.push_back(read_layer(neuron, l, fuse[l], dir));
     return n;
+}
+
+// ---- binary cache ---------------------------------------------------------
+constexpr char kCacheMagic[8] = {'C', 'S', 'P', 'D', 'N', 'N', 'C', '1'};
+
+// (size, mtime in ns) of every source file, in a fixed order; empty if one is missing
+inline std::vector<int64_t> source_signature(int neuron, int layers, const std::string &dir) {
+    std::vector<std::string> files = {input_path(neuron, dir), fuse_path(neuron, layers, dir)};
+    for (int l = 0; l < layers; ++l) files.push_back(layer_path(neuron, l, dir));
+    std::vector<int64_t> sig;
+    for (const auto &f : files) {
+        struct stat st;
+        if (stat(f.c_str(), &st) != 0) return {};
+        sig.push_back((int64_t)st.st_size);
+        sig.push_back((int64_t)st.st_mtim.tv_sec * 1000000000LL + st.st_mtim.tv_nsec);
+    }
+    return sig;
+}
+
+inline std::string cache_path(const std::string &cache_dir, int neuron, int batch, int layers) {
+    return cache_dir + "/cospdnn-n" + std::to_string(neuron) + "-b" + std::to_string(batch) + "-l" +
+           std::to_string(layers) + ".bin";
+}
+
+template <typename T>
+inline bool put(std::FILE *f, const T *p, size_t n) {
+    return n == 0 || std::fwrite(p, sizeof(T), n, f) == n;
+}
+template <typename T>
+inline bool get(std::FILE *f, T *p, size_t n) {
+    return n == 0 || std::fread(p, sizeof(T), n, f) == n;
+}
+
+inline bool write_cache(const std::string &path, const Network &n, const std::vector<int64_t> &sig) {
+    const std::string tmp = path + ".tmp" + std::to_string((long)getpid());
+    std::FILE *f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return false;
+    const int32_t hdr[4] = {n.neuron, n.batch, n.layers, n.input.integral ? 1 : 0};
+    const int64_t nsig = (int64_t)sig.size(), nread = n.input.read;
+    bool ok = put(f, kCacheMagic, 8) && put(f, hdr, 4) && put(f, &nsig, 1) && put(f, sig.data(), sig.size()) &&
+              put(f, &nread, 1);
+    if (n.input.integral) {
+        std::vector<uint8_t> b(n.input.rows.size());
+        for (size_t i = 0; i < b.size(); ++i) b[i] = (uint8_t)n.input.rows[i];
+        ok = ok && put(f, b.data(), b.size());
+    } else {
+        ok = ok && put(f, n.input.rows.data(), n.input.rows.size());
+    }
+    for (const auto &c : n.w) {
+        const int64_t nnz = (int64_t)c.rowidx.size();
+        ok = ok && put(f, &nnz, 1) && put(f, c.colptr.data(), c.colptr.size()) && put(f, c.rowidx.data(), c.rowidx.size()) &&
+             put(f, c.vals.data(), c.vals.size());
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (ok) ok = std::rename(tmp.c_str(), path.c_str()) == 0;
+    if (!ok) std::remove(tmp.c_str());
+    return ok;
+}
+
+// true when `path` holds this network and its header matches `sig`
+inline bool read_cache(const std::string &path, int neuron, int batch, int layers, const std::vector<int64_t> &sig,
+                       Network &n) {
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    char magic[8];
+    int32_t hdr[4];
+    int64_t nsig = 0;
+    bool ok = get(f, magic, 8) && std::memcmp(magic, kCacheMagic, 8) == 0 && get(f, hdr, 4) && hdr[0] == neuron &&
+              hdr[1] == batch && hdr[2] == layers && get(f, &nsig, 1) && nsig == (int64_t)sig.size();
+    std::vector<int64_t> old(ok ? (size_t)nsig : 0);
+    ok = ok && get(f, old.data(), old.size()) && old == sig;
+    int64_t nread = 0;
+    ok = ok && get(f, &nread, 1);
+    if (ok) {
+        n.neuron = neuron;
+        n.batch = batch;
+        n.layers = layers;
+        n.input.integral = hdr[3] != 0;
+        n.input.read = (long)nread;
+        n.input.rows.assign((size_t)batch * neuron, 0.0f);
+        if (n.input.integral) {
+            std::vector<uint8_t> b(n.input.rows.size());
+            ok = get(f, b.data(), b.size());
+            for (size_t i = 0; ok && i < b.size(); ++i) n.input.rows[i] = (float)b[i];
+        } else {
+            ok = get(f, n.input.rows.data(), n.input.rows.size());
+        }
+    }
+    for (int l = 0; ok && l < layers; ++l) {
+        Csc c;
+        int64_t nnz = -1;
+        ok = get(f, &nnz, 1) && nnz >= 0 && nnz <= (int64_t)neuron * neuron;
+        if (!ok) break;
+        c.colptr.resize(neuron + 1);
+        c.rowidx.resize((size_t)nnz);
+        c.vals.resize((size_t)nnz);
+        ok = get(f, c.colptr.data(), c.colptr.size()) && get(f, c.rowidx.data(), c.rowidx.size()) &&
+             get(f, c.vals.data(), c.vals.size()) && c.colptr[0] == 0 && c.colptr[neuron] == nnz;
+        for (int j = 0; ok && j < neuron; ++j) ok = c.colptr[j] <= c.colptr[j + 1];
+        for (int64_t t = 0; ok && t < nnz; ++t) ok = c.rowidx[t] >= 0 && c.rowidx[t] < neuron;
+        if (ok) n.w.push_back(std::move(c));
+    }
+    std::fclose(f);
+    if (!ok) n = Network();
+    return ok;
+}
+
+// The network from the TSV files, through the binary cache when COSPDNN_CACHE
+// names a directory.
+inline Network load_network(int neuron, int batch, int layers, const std::string &dir) {
+    const char *cdir = std::getenv("COSPDNN_CACHE");
+    if (!cdir || !*cdir) return parse_network(neuron, batch, layers, dir);
+    const std::string path = cache_path(cdir, neuron, batch, layers);
+    const auto sig = source_signature(neuron, layers, dir);
+    Network n;
+    if (!sig.empty() && read_cache(path, neuron, batch, layers, sig, n)) {
+        std::cout << "Read cache success! file = " << path << std::endl;
+        return n;
+    }
+    n = parse_network(neuron, batch, layers, dir);
+    if (!sig.empty() && !write_cache(path, n, sig)) std::cout << "cache not written: " << path << std::endl;
+    return n;
+}
+
+// ---- categories -------------------------------------------------------------
+// 0-based surviving rows -> file of 1-based ids, one per line
+inline bool write_categories(const std::string &path, const std::vector<int64_t> &cats0) {
+    std::ofstream f(path);
+    if (!f) return false;
+    for (int64_t c : cats0) f << c + 1 << "\n";
+    return (bool)f;
+}
+
+// 1-based ids of a categories file; false when it cannot be read or holds
+// anything but positive integers
+inline bool read_categories(const std::string &path, std::vector<int64_t> &ids) {
+    std::ifstream f(path);
+    if (!f) return false;
+    ids.clear();
+    std::string tok;
+    while (f >> tok) {
+        char *end = nullptr;
+        const long long v = std::strtoll(tok.c_str(), &end, 10);
+        if (end == tok.c_str() || *end != '\0' || v < 1) return false;
+        ids.push_back(v);
+    }
+    return true;
+}
+
+struct CategoryCheck {
+    size_t ours = 0, truth = 0, missing = 0, extra = 0;
+    bool ok() const { return missing == 0 && extra == 0; }
+};
+
+// ours0: 0-based rows; truth1: 1-based ids
+inline CategoryCheck compare_categories(const std::vector<int64_t> &ours0, std::vector<int64_t> truth1) {
+    std::vector<int64_t> ours1(ours0.size());
+    for (size_t i = 0; i < ours0.size(); ++i) ours1[i] = ours0[i] + 1;
+    std::sort(ours1.begin(), ours1.end());
+    ours1.erase(std::unique(ours1.begin(), ours1.end()), ours1.end());
+    std::sort(truth1.begin(), truth1.end());
+    truth1.erase(std::unique(truth1.begin(), truth1.end()), truth1.end());
+    std::vector<int64_t> d;
+    CategoryCheck r;
+    r.ours = ours1.size();
+    r.truth = truth1.size();
+    std::set_difference(truth1.begin(), truth1.end(), ours1.begin(), ours1.end(), std::back_inserter(d));
+    r.missing = d.size();
+    d.clear();
+    std::set_difference(ours1.begin(), ours1.end(), truth1.begin(), truth1.end(), std::back_inserter(d));
+    r.extra = d.size();
+    return r;
+}
+
+// Writes and checks the categories as the environment asks; returns 0, or 2
+// when a truth file was given and does not match.
+inline int report_categories(const std::vector<int64_t> &cats0, const char *out_env, const char *truth_env,
+                             const std::string &label) {
+    const char *out = std::getenv(out_env);
+    if (out && *out) {
+        if (!write_categories(out, cats0)) die(std::string("cannot write ") + out);
+        std::cout << label << "categories written: " << out << std::endl;
+    }
+    const char *truth = std::getenv(truth_env);
+    if (!truth || !*truth) return 0;
+    std::vector<int64_t> t;
+    if (!read_categories(truth, t)) die(std::string("cannot read truth file ") + truth);
+    const CategoryCheck r = compare_categories(cats0, t);
+    std::cout << label << "categories check: " << (r.ok() ? "PASS" : "FAIL") << " (ours " << r.ours << ", truth "
+              << r.truth << ", missing " << r.missing << ", extra " << r.extra << ")" << std::endl;
+    return r.ok() ? 0 : 2;
 }
 
 // Adds rows [r0, r1) of `net` to engine `e`; returns the net id.

@@ -59,15 +59,29 @@ def test_cli_single_matches_oracle(tmp_path):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
+    from cospdnn_b200 import categories as cat
     ref = _dataset(tmp_path, 1024, 6, 500, 43, 0)
-    for prec in ("fp16", "fp32"):
-        env = dict(os.environ, COSPDNN_PRECISION=prec)
+    truth = tmp_path / "truth.tsv"
+    cat.write(truth, ref["categories"])
+    (tmp_path / "cache").mkdir()
+    for prec in ("fp16", "fp32", "fp16"):  # the second fp16 run reads the binary cache
+        ours = tmp_path / f"ours-{prec}.tsv"
+        env = dict(os.environ, COSPDNN_PRECISION=prec, COSPDNN_CATEGORIES=str(ours), COSPDNN_TRUTH=str(truth),
+                   COSPDNN_CACHE=str(tmp_path / "cache"))
         out = subprocess.run([_exe("cospdnn"), "1024", "500", "6", "1", "0", str(tmp_path)],
                              capture_output=True, text=True, timeout=600, env=env)
         assert out.returncode == 0, out.stdout + out.stderr
         assert _alive(out.stdout, "") == list(ref["alive"])
         assert "Kernel Exec Time = " in out.stdout
         assert f"[Categories] :{len(ref['categories'])}" in out.stdout
+        assert "categories check: PASS" in out.stdout
+        assert cat.read(ours).tolist() == list(ref["categories"])
+    assert "Read cache success" in out.stdout
+    # a truth file that differs: FAIL and exit status 2
+    cat.write(truth, list(ref["categories"])[1:])
+    out = subprocess.run([_exe("cospdnn"), "1024", "500", "6", "1", "0", str(tmp_path)],
+                         capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 2 and "categories check: FAIL" in out.stdout and "extra 1" in out.stdout
 
 
 @pytest.mark.gpu
@@ -77,9 +91,17 @@ def test_cli_double_matches_oracle(tmp_path):
         pytest.skip("no CUDA device")
     ref1 = _dataset(tmp_path, 1024, 5, 400, 47, 0)
     ref2 = _dataset(tmp_path, 2048, 7, 300, 53, 1)
+    from cospdnn_b200 import categories as cat
+    env = dict(os.environ)
+    for i, r in ((1, ref1), (2, ref2)):
+        cat.write(tmp_path / f"truth{i}.tsv", r["categories"])
+        env[f"COSPDNN_TRUTH_{i}"] = str(tmp_path / f"truth{i}.tsv")
+        env[f"COSPDNN_CATEGORIES_{i}"] = str(tmp_path / f"ours{i}.tsv")
     out = subprocess.run([_exe("cospdnn_double"), "1024", "400", "5", "2048", "300", "7", "0", str(tmp_path)],
-                         capture_output=True, text=True, timeout=600)
+                         capture_output=True, text=True, timeout=600, env=env)
     assert out.returncode == 0, out.stdout + out.stderr
     assert _alive(out.stdout, "SpDNN 1 ") == list(ref1["alive"])
     assert _alive(out.stdout, "SpDNN 2 ") == list(ref2["alive"])
     assert "Total Kernel Exec Time = " in out.stdout
+    assert "SpDNN 1 categories check: PASS" in out.stdout and "SpDNN 2 categories check: PASS" in out.stdout
+    assert cat.read(tmp_path / "ours2.tsv").tolist() == list(ref2["categories"])

@@ -1,0 +1,153 @@
+"""Host-side parts of the command lines, on CPU: the binary dataset cache
+(COSPDNN_CACHE) and the categories files (COSPDNN_CATEGORIES, COSPDNN_TRUTH),
+through a small program built with g++ against cospdnn_b200/cli/reference_io.h,
+and the Python categories module (cospdnn_b200.categories)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from netgen import make_net
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+HARNESS = r"""
+#include <cinttypes>
+#include "reference_io.h"
+using namespace cospdnn_cli;
+
+static uint64_t mix(uint64_t h, const void *p, size_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+static uint64_t digest(const Network &n) {
+    uint64_t h = 1469598103934665603ull;
+    h = mix(h, n.input.rows.data(), n.input.rows.size() * sizeof(float));
+    for (const auto &c : n.w) {
+        h = mix(h, c.colptr.data(), c.colptr.size() * 4);
+        h = mix(h, c.rowidx.data(), c.rowidx.size() * 4);
+        h = mix(h, c.vals.data(), c.vals.size() * 4);
+    }
+    return h;
+}
+int main(int argc, char **argv) {
+    const std::string mode = argv[1];
+    if (mode == "load" || mode == "parse") {
+        const int n = atoi(argv[2]), b = atoi(argv[3]), l = atoi(argv[4]);
+        const Network net = mode == "load" ? load_network(n, b, l, argv[5]) : parse_network(n, b, l, argv[5]);
+        printf("digest %" PRIu64 " integral %d read %ld layers %zu\n", digest(net), (int)net.input.integral,
+               net.input.read, net.w.size());
+        return 0;
+    }
+    std::vector<int64_t> rows;
+    for (int i = 2; i < argc; ++i) rows.push_back(atoll(argv[i]));
+    return report_categories(rows, "COSPDNN_CATEGORIES", "COSPDNN_TRUTH", "");
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not found")
+    d = tmp_path_factory.mktemp("harness")
+    src = d / "h.cpp"
+    src.write_text(HARNESS)
+    exe = d / "h"
+    subprocess.run([gxx, "-O1", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), "-I",
+                    os.path.join(ROOT, "cospdnn_b200", "cli"), str(src), "-o", str(exe)], check=True)
+    return str(exe)
+
+
+def _run(exe, args, env=None):
+    out = subprocess.run([exe] + [str(a) for a in args], capture_output=True, text=True, timeout=120,
+                         env=dict(os.environ, **(env or {})))
+    return out.returncode, out.stdout
+
+
+def _digest(text):
+    line = [x for x in text.splitlines() if x.startswith("digest ")][0]
+    return line.split()[1]
+
+
+def test_binary_cache(harness, tmp_path):
+    from cospdnn_b200 import synth
+    n, L, rows = 256, 4, 60
+    data = tmp_path / "data"
+    csc, y0, _ = make_net(n, L, rows, seed=71, dlo=0.2, dhi=0.4)
+    rng = np.random.default_rng(71)
+    fuse = [rng.permutation(n).astype(np.int32) for _ in range(L)]
+    synth.write_reference_dataset(str(data), n, L, y0, csc, fuse=fuse)
+    cache = tmp_path / "cache"
+    cache.mkdir()
+    env = {"COSPDNN_CACHE": str(cache)}
+    rc, parsed = _run(harness, ["parse", n, rows, L, data])
+    assert rc == 0 and "layers 4" in parsed and "integral 1" in parsed
+    # first load parses and writes the cache, the second reads it
+    rc, first = _run(harness, ["load", n, rows, L, data], env)
+    assert rc == 0 and "Read cache success" not in first
+    cfile = cache / f"cospdnn-n{n}-b{rows}-l{L}.bin"
+    assert cfile.exists()
+    rc, second = _run(harness, ["load", n, rows, L, data], env)
+    assert rc == 0 and "Read cache success" in second
+    assert _digest(first) == _digest(second) == _digest(parsed)
+    # a changed source file invalidates the cache
+    lay = data / f"neuron{n}" / f"{n}-l2.tsv"
+    text = lay.read_text().splitlines()
+    a, b, v = text[0].split("\t")
+    text[0] = f"{a}\t{b}\t0.5"
+    lay.write_text("\n".join(text) + "\n")
+    rc, changed = _run(harness, ["load", n, rows, L, data], env)
+    assert rc == 0 and "Read cache success" not in changed
+    _, reparsed = _run(harness, ["parse", n, rows, L, data])
+    assert _digest(changed) == _digest(reparsed) != _digest(parsed)
+    rc, again = _run(harness, ["load", n, rows, L, data], env)
+    assert "Read cache success" in again and _digest(again) == _digest(reparsed)
+    # a damaged cache falls back to the files
+    cfile.write_bytes(cfile.read_bytes()[:100])
+    rc, damaged = _run(harness, ["load", n, rows, L, data], env)
+    assert rc == 0 and "Read cache success" not in damaged and _digest(damaged) == _digest(reparsed)
+    # another batch is another cache entry
+    rc, fewer = _run(harness, ["load", n, rows - 10, L, data], env)
+    assert rc == 0 and (cache / f"cospdnn-n{n}-b{rows - 10}-l{L}.bin").exists()
+
+
+def test_categories_cli_helpers(harness, tmp_path):
+    out, truth = tmp_path / "ours.tsv", tmp_path / "truth.tsv"
+    truth.write_text("3\n1\n10\n")
+    env = {"COSPDNN_CATEGORIES": str(out), "COSPDNN_TRUTH": str(truth)}
+    rc, text = _run(harness, ["cats", 0, 2, 9], env)
+    assert rc == 0 and "categories check: PASS (ours 3, truth 3, missing 0, extra 0)" in text
+    assert out.read_text() == "1\n3\n10\n"
+    rc, text = _run(harness, ["cats", 0, 2, 8], env)
+    assert rc == 2 and "FAIL (ours 3, truth 3, missing 1, extra 1)" in text
+    rc, text = _run(harness, ["cats"], env)  # no survivors
+    assert rc == 2 and "missing 3, extra 0" in text and out.read_text() == ""
+    truth.write_text("1\nx\n")
+    rc, text = _run(harness, ["cats", 0], env)
+    assert rc != 0 and "cannot read truth file" in text
+
+
+def test_categories_module(tmp_path):
+    from cospdnn_b200 import categories as cat
+    p = tmp_path / "c.tsv"
+    cat.write(p, [9, 0, 2, 2])
+    assert p.read_text() == "1\n3\n10\n"
+    assert cat.read(p).tolist() == [0, 2, 9]
+    r = cat.check([0, 2, 9], p)
+    assert r["ok"] and r["ours"] == 3 and r["truth"] == 3
+    r = cat.check([0, 2, 8], p)
+    assert not r["ok"] and r["missing"].tolist() == [9] and r["extra"].tolist() == [8]
+    q = tmp_path / "d.tsv"
+    cat.write(q, [0, 2, 9])
+    assert cat.main([str(q), str(p)]) == 0
+    cat.write(q, [0, 2])
+    assert cat.main([str(q), str(p)]) == 2
+    bad = tmp_path / "bad.tsv"
+    bad.write_text("0\n")
+    with pytest.raises(ValueError):
+        cat.read(bad)
