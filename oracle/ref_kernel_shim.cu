@@ -29,7 +29,8 @@ extern "C" int ref_cospdnn_single(const void *A, const void *B, float *C, const 
 
 // Runs test_graph_challenge_tc on one GPU.  y0: [batch][neuron] bytes (binary
 // images); per layer l: values[l] (nval[l] floats), row_index[l] (nrow[l]),
-// col_ptr[l] (ncol[l]); identity fuse.  Returns the reference's own printed
+// col_ptr[l] (ncol[l]); fuse_rows[l] (neuron ints: the activation row block
+// row r of layer l reads), or the identity when fuse_rows is NULL.  Returns the reference's own printed
 // "Kernel Exec Time" in *kernel_ms, the wall time of the call in *wall_ms,
 // the last "feature = " count it printed in *last_feature, and every printed
 // "layer l, feature = n" count in features[l] (the reference prints these for
@@ -40,7 +41,7 @@ extern "C" int ref_run_network(const uint8_t *y0, int batch, int neuron, int lay
                                const int *const *col_ptr, const int64_t *ncol, float bias,
                                double *kernel_ms, double *wall_ms, int *last_feature,
                                int *features, int max_features, char *log_tail,
-                               int log_tail_len) {
+                               int log_tail_len, const int *const *fuse_rows) {
     std::vector<std::vector<float>> input(batch, std::vector<float>(neuron));
     for (int b = 0; b < batch; ++b)
         for (int j = 0; j < neuron; ++j) input[b][j] = (float)y0[(int64_t)b * neuron + j];
@@ -53,7 +54,7 @@ extern "C" int ref_run_network(const uint8_t *y0, int batch, int neuron, int lay
     }
     std::vector<std::vector<int>> fuse(layers + 1, std::vector<int>(neuron));
     for (int l = 0; l <= layers; ++l)
-        for (int j = 0; j < neuron; ++j) fuse[l][j] = j;
+        for (int j = 0; j < neuron; ++j) fuse[l][j] = (fuse_rows && l < layers) ? fuse_rows[l][j] : j;
 
     std::stringstream captured;
     std::streambuf *old = std::cout.rdbuf(captured.rdbuf());

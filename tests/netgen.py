@@ -100,3 +100,35 @@ def make_random_net(neuron, layers, rows, seed=1, dlo=0.2, dhi=0.4, bias=-0.2, *
     csc = [random_layer(neuron, seed, l, **kw) for l in range(layers)]
     y0 = po.input_binary(seed, 0, rows, neuron, dlo, dhi)
     return csc, y0, np.float32(bias)
+
+
+def shift_half_block_layer(neuron, seed, layer, val=0.125):
+    """Like half_block_layer with output block column g reading the first 8
+    rows of input blocks (g + a) and (g + b) mod N/16 (2(a - b) != 0 mod
+    N/16), so no two input row groups feed the same pair of block columns."""
+    nb = neuron // 16
+    g = SplitMix(seed * 7919 + layer)
+    while True:
+        a, b = g.next() % nb, g.next() % nb
+        if a != b and (2 * (a - b)) % nb != 0:
+            break
+    colptr = np.zeros(neuron + 1, np.int32)
+    rowidx = []
+    for j in range(neuron):
+        blk, r = divmod(j, 16)
+        ins = []
+        if r < 8:
+            for s in sorted([(blk + a) % nb, (blk + b) % nb]):
+                ins += [16 * s + k for k in range(8)]
+        rowidx += ins
+        colptr[j + 1] = colptr[j] + len(ins)
+    return colptr, np.array(rowidx, np.int32), np.full(len(rowidx), val, np.float32)
+
+
+def permute_rows(csc, neuron, seed):
+    """The layer with its input rows renamed by a seeded permutation (a
+    different network with the same hidden block structure)."""
+    cp, ri, vv = csc
+    col = np.repeat(np.arange(neuron), np.diff(cp))
+    perm = np.random.default_rng(seed).permutation(neuron)
+    return po.coo_to_csc(perm[np.asarray(ri)], col, np.asarray(vv, np.float32), neuron)

@@ -116,6 +116,23 @@ def test_binary_cache(harness, tmp_path):
     assert rc == 0 and (cache / f"cospdnn-n{n}-b{rows - 10}-l{L}.bin").exists()
 
 
+def test_reordered_dataset_same_product(harness, tmp_path):
+    """cospdnn_b200.reorder rewrites the weights and the fuse matrix; the
+    command lines fold the fuse back into W, so both datasets give the same
+    network."""
+    from cospdnn_b200 import reorder, synth
+    from netgen import permute_rows, shift_half_block_layer
+    n, L, rows = 1024, 3, 40
+    layers = [permute_rows(shift_half_block_layer(n, 17, l), n, 170 + l) for l in range(L)]
+    y0 = (np.random.default_rng(17).random((rows, n)) < 0.2).astype(np.uint8)
+    synth.write_reference_dataset(str(tmp_path / "src"), n, L, y0, layers)
+    stats = reorder.reorder_dataset(str(tmp_path / "src"), str(tmp_path / "dst"), n, L)
+    assert all(b < a for a, b in stats)
+    _, src = _run(harness, ["parse", n, rows, L, tmp_path / "src"])
+    _, dst = _run(harness, ["parse", n, rows, L, tmp_path / "dst"])
+    assert _digest(src) == _digest(dst)
+
+
 def test_categories_cli_helpers(harness, tmp_path):
     out, truth = tmp_path / "ours.tsv", tmp_path / "truth.tsv"
     truth.write_text("3\n1\n10\n")

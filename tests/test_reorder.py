@@ -1,0 +1,92 @@
+"""The similarity reordering (cospdnn_b200.reorder) on CPU: it recovers hidden
+block structure (rows of dense-block layers renamed by a permutation) down to
+the aligned blocks the reference's greedy builder makes for the unpermuted
+layer, never increases the block count, keeps the product (W' read through
+the fuse row equals W), and its block count is the reference builder's."""
+import numpy as np
+import pytest
+
+from netgen import half_block_layer, permute_rows, random_layer, shift_half_block_layer
+from cospdnn_b200 import reorder as ro
+
+
+def _fold(csc, fuse, n, oracle):
+    """W[fuse[u']][v] = W'[u'][v]: the product the reference computes."""
+    row, col, val = oracle.csc_to_coo(*csc)
+    return oracle.coo_to_csc(np.asarray(fuse)[row], col, val, n)
+
+
+def _same(a, b):
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("n,seed", [(1024, 3), (4096, 8)])
+def test_hidden_r1_blocks_recovered(oracle, n, seed):
+    layer = oracle.masks_to_csc(oracle.r1_masks(seed, 0, 0, n), n)
+    hidden = permute_rows(layer, n, seed)
+    order, csc, before, after = ro.reorder_layer(*hidden, n)
+    row, col, val = oracle.csc_to_coo(*csc)
+    bcp, bri, _, _ = oracle.bcsc_greedy(row, col, val, 16)
+    assert np.all(np.diff(bcp) == 2) and np.all(bri % 16 == 0)
+    assert after == len(bri) == 2 * (n // 16) < before
+    _same(_fold(csc, order, n, oracle), hidden)
+
+
+def test_shifted_half_blocks_two_aligned_blocks(oracle):
+    n = 1024
+    for l in range(4):
+        hidden = permute_rows(shift_half_block_layer(n, 5, l), n, 50 + l)
+        order, csc, before, after = ro.reorder_layer(*hidden, n)
+        row, col, val = oracle.csc_to_coo(*csc)
+        bcp, bri, _, _ = oracle.bcsc_greedy(row, col, val, 16)
+        assert np.all(np.diff(bcp) == 2) and np.all(bri % 16 == 0) and after < before
+        # the non-zeros sit in the first 8 rows of each block (offsets 0..7)
+        assert np.all(np.isin(row % 16, np.arange(8)))
+        _same(_fold(csc, order, n, oracle), hidden)
+
+
+def test_xor_half_blocks_merge(oracle):
+    """Under XOR structure the two row groups of a column have equal
+    signatures and share one aligned block: one block per column."""
+    n = 1024
+    hidden = permute_rows(half_block_layer(n, 2, 0, 0), n, 7)
+    order, csc, before, after = ro.reorder_layer(*hidden, n)
+    assert after == n // 16 < before
+    _same(_fold(csc, order, n, oracle), hidden)
+
+
+@pytest.mark.parametrize("kind", ["xor", "random", "r1"])
+def test_never_more_blocks_and_count_matches_builder(oracle, kind):
+    n = 1024
+    for l in range(3):
+        if kind == "xor":
+            layer = oracle.masks_to_csc(oracle.xor_masks(11, 0, l, n), n)
+        elif kind == "random":
+            layer = random_layer(n, 11, l)
+        else:
+            layer = oracle.masks_to_csc(oracle.r1_masks(11, 0, l, n), n)
+        row, col, val = oracle.csc_to_coo(*layer)
+        assert ro.greedy_blocks(row, col, n) == len(oracle.bcsc_greedy(row, col, val, 16)[1])
+        order, csc, before, after = ro.reorder_layer(*layer, n)
+        assert after <= before
+        if after == before:
+            np.testing.assert_array_equal(order, np.arange(n))
+        r2, c2, v2 = oracle.csc_to_coo(*csc)
+        assert ro.greedy_blocks(r2, c2, n) == len(oracle.bcsc_greedy(r2, c2, v2, 16)[1]) == after
+        _same(_fold(csc, order, n, oracle), layer)
+
+
+def test_reorder_network_and_main(oracle, tmp_path, capsys):
+    from cospdnn_b200 import synth
+    n, L = 1024, 3
+    layers = [permute_rows(shift_half_block_layer(n, 9, l), n, 90 + l) for l in range(L)]
+    out, fuse, stats = ro.reorder_network(layers, n)
+    assert len(out) == len(fuse) == L and all(b < a for a, b in stats)
+    y0 = (np.random.default_rng(1).random((20, n)) < 0.2).astype(np.uint8)
+    synth.write_reference_dataset(str(tmp_path / "src"), n, L, y0, layers)
+    assert ro.main([str(tmp_path / "src"), str(tmp_path / "dst"), str(n), str(L)]) == 0
+    assert "greedy 16x16 blocks:" in capsys.readouterr().out
+    f = np.loadtxt(tmp_path / "dst" / "fuse_matrix" / f"neuron{n}" / f"{n}_{L}_fuse.tsv", dtype=np.int64)
+    for l in range(L):
+        np.testing.assert_array_equal(f[l], fuse[l])
