@@ -1,0 +1,355 @@
+// Layer 0 by bit counting.  The inputs of the sparse-DNN benchmarks are binary
+// images and every output's weights are one value (1/16 in the Graph
+// Challenge networks), so an output of layer 0 is
+//     z = bias + w_j * (number of its inputs that are 1),
+// an exact integer count.  The kernel counts 32 rows at once: the inputs are
+// stored as bit planes (one 32-bit word per feature and 32 rows, built with
+// the rest of the input conversion), a CTA stages one unit of 32 rows (4
+// bytes per feature) in shared memory, and lane j of a warp adds the words
+// of output j's inputs into six bit-sliced counters (carry-save adders,
+// Harley-Seal: about 2.4 logic instructions per word for 32 rows).  The
+// counts are moved into bytes four rows at a time (a multiply spreads 4 bits
+// of a plane into 4 bytes), then bias, clamp and the store in the compute
+// type follow the row-tile kernel's epilogue, with the same per-row
+// statistics for the keep/prune decision.  Shared-memory traffic per output
+// and 32 rows is 32 words against 32 * 32 rows of 16-bit values in the
+// general kernel.
+//
+// Entry schedule: the 32 outputs of a warp read their inputs' words at
+// step t from 32 distinct banks (edge colouring of outputs x banks, as in the
+// row-tile kernel), padded with zero words placed in the free banks.
+// Binary inputs are checked per input (U8 maxima, the packed-bit format is
+// binary); otherwise, and for FP32 input values, layer 0 runs on the general
+// kernel.
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+
+#include "bits_layer.cuh"
+#include "cc_layer.cuh"
+
+namespace cospdnn {
+
+namespace {
+
+constexpr int kBitsThreads = 256;
+constexpr int kBitsWarps = kBitsThreads / 32;
+constexpr int kBitsMaxK = 63;  // six bit-sliced counters
+
+__device__ __forceinline__ void csa(uint32_t &h, uint32_t &l, uint32_t a, uint32_t b, uint32_t c) {
+    const uint32_t u = a ^ b;
+    h = (a & b) | (u & c);
+    l = u ^ c;
+}
+
+// count += number of set bits among x[0..7] at every bit position
+__device__ __forceinline__ void add8(uint32_t (&p)[6], const uint32_t (&x)[8]) {
+    uint32_t twosA, twosB, foursA, foursB, eightsA;
+    csa(twosA, p[0], p[0], x[0], x[1]);
+    csa(twosB, p[0], p[0], x[2], x[3]);
+    csa(foursA, p[1], p[1], twosA, twosB);
+    csa(twosA, p[0], p[0], x[4], x[5]);
+    csa(twosB, p[0], p[0], x[6], x[7]);
+    csa(foursB, p[1], p[1], twosA, twosB);
+    csa(eightsA, p[2], p[2], foursA, foursB);
+    const uint32_t c8 = p[3] & eightsA;
+    p[3] ^= eightsA;
+    const uint32_t c16 = p[4] & c8;
+    p[4] ^= c8;
+    p[5] ^= c16;  // counts stay below 64
+}
+
+// Counts of rows 4q..4q+3, one per byte.
+__device__ __forceinline__ uint32_t counts4(const uint32_t (&p)[6], int q) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) {
+        const uint32_t nib = (p[b] >> (4 * q)) & 0xFu;
+        c |= (nib * (0x00204081u << b)) & (0x01010101u << b);  // bit i of nib -> bit b of byte i
+    }
+    return c;
+}
+
+template <typename T>
+struct Pack;
+template <>
+struct Pack<float> {
+    static constexpr int kPer16 = 4;
+};
+template <>
+struct Pack<__half> {
+    static constexpr int kPer16 = 8;
+};
+template <>
+struct Pack<__nv_bfloat16> {
+    static constexpr int kPer16 = 8;
+};
+
+__device__ __forceinline__ bool l0_net(const NetDev &nd, int prec) {
+    return nd.l0_k > 0 && nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 4 && nd.prec == prec &&
+           !nd.st->done && nd.st->layer == 0 && nd.y0bits != nullptr && *nd.y0nonbin == 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBitsThreads, 2)
+    k_layer0_bits(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
+    count_launch(launches);
+    extern __shared__ uint4 l0_smem[];
+    uint32_t *s_bits = reinterpret_cast<uint32_t *>(l0_smem);
+    __shared__ uint32_t s_zmax[32], s_zdist[32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int n = 0; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        if (!l0_net(nd, prec)) continue;
+        if (blockIdx.x == 0 && threadIdx.x == 0) nd.st->l0_bits = 1;  // the row-tile kernel skips layer 0
+        const int N = nd.N, R = nd.st->R, TR = nd.layout, K8 = nd.l0_k / 8;
+        const int units = (R + 31) / 32, ngroups = N / 32;
+        const LayerDev &lw = nd.layers[0];
+        T *out = (T *)nd.act[nd.st->in_buf ^ 1];
+        const float bias = nd.bias;
+        for (int u = blockIdx.x; u < units; u += gridDim.x) {
+            __syncthreads();  // the previous unit is done with the words and the row statistics
+            {
+                const uint4 *src = reinterpret_cast<const uint4 *>(nd.y0bits + (int64_t)u * N);
+                for (int i = threadIdx.x; i < N / 4; i += kBitsThreads) l0_smem[i] = __ldg(src + i);
+                if (threadIdx.x < 32) {
+                    s_bits[N + threadIdx.x] = 0u;  // padding words, one per bank
+                    s_zmax[threadIdx.x] = 0u;
+                    s_zdist[threadIdx.x] = 0x7F800000u;
+                }
+            }
+            __syncthreads();
+            float zmx[32], zds[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                zmx[r] = -INFINITY;
+                zds[r] = INFINITY;
+            }
+            for (int g = warp; g < ngroups; g += kBitsWarps) {
+                const int j = g * 32 + lane;
+                uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+                const uint4 *ent = nd.l0_idx + (int64_t)g * K8 * 32 + lane;
+                for (int t = 0; t < K8; ++t) {
+                    const uint4 q = __ldg(ent + (int64_t)t * 32);
+                    const uint32_t x[8] = {s_bits[q.x & 0xFFFFu], s_bits[q.x >> 16], s_bits[q.y & 0xFFFFu],
+                                           s_bits[q.y >> 16],     s_bits[q.z & 0xFFFFu], s_bits[q.z >> 16],
+                                           s_bits[q.w & 0xFFFFu], s_bits[q.w >> 16]};
+                    add8(p, x);
+                }
+                const float w = nd.l0_w[j];
+                // the 32 rows' values (row r = 4q + k), then the stores
+                constexpr int V = Pack<T>::kPer16;  // values per 16-byte piece
+                __align__(16) T ov[32];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const uint32_t c4 = counts4(p, q);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * q + k;
+                        const float z = fmaf((float)((c4 >> (8 * k)) & 0xFFu), w, bias);
+                        zmx[r] = fmaxf(zmx[r], z);
+                        zds[r] = fminf(zds[r], fabsf(z - 16.0f));
+                        ov[r] = act_traits<T>::from_f(clamp32(z));
+                    }
+                }
+                const int64_t row0 = (int64_t)u * 32;
+#pragma unroll
+                for (int k = 0; k < 32 / V; ++k) {
+                    if (TR >= V) {  // a 16-byte piece lies inside one tile
+                        *reinterpret_cast<uint4 *>(out + act_index(TR, N, row0 + k * V, j)) =
+                            *reinterpret_cast<const uint4 *>(ov + k * V);
+                    } else {  // 16-bit values, tiles of 4 rows: two 8-byte pieces
+                        *reinterpret_cast<uint2 *>(out + act_index(TR, N, row0 + k * V, j)) =
+                            *reinterpret_cast<const uint2 *>(ov + k * V);
+                        *reinterpret_cast<uint2 *>(out + act_index(TR, N, row0 + k * V + 4, j)) =
+                            *reinterpret_cast<const uint2 *>(ov + k * V + 4);
+                    }
+                }
+            }
+            // row statistics: over the warp's outputs, then over the CTA
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
+                const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
+                if (lane == r) {
+                    atomicMax(&s_zmax[r], m);
+                    atomicMin(&s_zdist[r], d);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                const int p = u * 32 + threadIdx.x;
+                if (p < R) {
+                    const double steps = fast_steps(nd, lw);
+                    const float ez = z_error_bound(nd.err[0][p], nd.mx[0][p], lw.S, lw.dW, bias, steps);
+                    float em, ym;
+                    const float zm = ord2f(s_zmax[threadIdx.x]);
+                    const float zd = __uint_as_float(s_zdist[threadIdx.x]);
+                    const float c = clamp32(zm);
+                    ym = act_traits<T>::to_f(act_traits<T>::from_f(c));
+                    // as the row-tile kernel (row_stats): outputs within 16 + ez of 16
+                    // carry the bound plus their storage rounding
+                    float se = 0.0f;
+                    if constexpr (sizeof(T) == 2) {
+                        se = std::is_same<T, __half>::value ? __fmaf_ru(c, 4.8828125e-04f, 2.98023224e-08f)
+                                                            : __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
+                    }
+                    em = zd < 16.0f + ez ? __fadd_ru(ez, se) : 0.0f;
+                    atomicMax(&nd.stat[3 * p], s_zmax[threadIdx.x]);
+                    atomicMax(&nd.stat[3 * p + 1], __float_as_uint(em));
+                    atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));
+                }
+            }
+        }
+    }
+}
+
+// Bit planes of U8 (FMT 0) or packed-bit (FMT 2) rows: one warp per
+// (unit of 32 rows, 32 features); lane r reads row 32*unit + r.
+template <int FMT>
+__global__ void k_convert_bits(const uint8_t *__restrict__ src, int rows, int N, uint32_t *__restrict__ bits) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int units = (rows + 31) / 32, fgroups = N / 32;
+    for (int64_t t = w; t < (int64_t)units * fgroups; t += nw) {
+        const int u = (int)(t / fgroups), fg = (int)(t % fgroups);
+        const int64_t row = (int64_t)u * 32 + lane;
+        uint32_t mine = 0;  // bit k = feature 32*fg + k of this lane's row
+        if (row < rows) {
+            if (FMT == COSPDNN_INPUT_BITS) {
+                const uint8_t *b = src + row * (N / 8) + fg * 4;
+                mine = (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+            } else {
+                const uint8_t *b = src + row * N + fg * 32;
+#pragma unroll
+                for (int k = 0; k < 32; k += 8) {
+                    const uint2 v = *reinterpret_cast<const uint2 *>(b + k);  // N % 32 == 0: 8-byte aligned
+                    const uint32_t lo = v.x, hi = v.y;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        mine |= (((lo >> (8 * i)) & 0xFFu) ? 1u : 0u) << (k + i);
+                        mine |= (((hi >> (8 * i)) & 0xFFu) ? 1u : 0u) << (k + 4 + i);
+                    }
+                }
+            }
+        }
+        // transpose: feature k's word has bit lane set when this lane's row has it
+        uint32_t outw = 0;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, (mine >> k) & 1u);
+            if (lane == k) outw = bal;
+        }
+        bits[(int64_t)u * N + fg * 32 + lane] = outw;
+    }
+}
+
+}  // namespace
+
+int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
+             int N, int prec, int TR, NetDev &nd, std::vector<void *> &owned) {
+    nd.l0_k = 0;
+    nd.l0_idx = nullptr;
+    nd.l0_w = nullptr;
+    if (TR < 4 || N % 32 != 0 || N + 32 > 65535) return 0;
+    // one weight value per output, at most 63 non-zero entries
+    std::vector<float> w(N, 0.0f);
+    std::vector<std::vector<int>> ent(N);
+    for (int j = 0; j < N; ++j) {
+        bool first = true;
+        for (int p = colptr[j]; p < colptr[j + 1]; ++p) {
+            if (vals[p] == 0.0f) continue;
+            if (first) {
+                w[j] = vals[p];
+                first = false;
+            } else if (vals[p] != w[j]) {
+                return 0;
+            }
+            ent[j].push_back(rowidx[p]);
+        }
+        if ((int)ent[j].size() > kBitsMaxK) return 0;
+    }
+    // weights in the compute type (what the error bound's dW assumes)
+    for (int j = 0; j < N; ++j) {
+        if (prec == COSPDNN_PREC_FP16) w[j] = __half2float(__float2half_rn(w[j]));
+        else if (prec == COSPDNN_PREC_BF16) w[j] = __bfloat162float(__float2bfloat16_rn(w[j]));
+    }
+    // per warp of 32 outputs: edge colouring outputs x banks
+    const int ngroups = N / 32;
+    std::vector<std::vector<int>> order(N);
+    int K = 1;
+    std::vector<int> eu, es, colour;
+    for (int g = 0; g < ngroups; ++g) {
+        eu.clear();
+        es.clear();
+        std::vector<int> ei;
+        for (int l = 0; l < 32; ++l)
+            for (int i : ent[g * 32 + l]) {
+                eu.push_back(l);
+                es.push_back(i % 32);
+                ei.push_back(i);
+            }
+        const int D = ei.empty() ? 0 : colour_group(32, eu, es, colour);
+        K = std::max(K, D);
+        for (int l = 0; l < 32; ++l) order[g * 32 + l].assign(D, -1);
+        for (size_t e = 0; e < ei.size(); ++e) order[g * 32 + eu[e]][colour[e]] = ei[e];
+    }
+    if (K > kBitsMaxK) return 0;
+    const int Kp = (K + 7) / 8 * 8;
+    // [group][step/8][lane] uint4 = 8 indices of 16 bits
+    std::vector<uint16_t> idx((size_t)ngroups * Kp * 32);
+    for (int g = 0; g < ngroups; ++g)
+        for (int t = 0; t < Kp; ++t) {
+            uint32_t used = 0;
+            for (int l = 0; l < 32; ++l) {
+                const auto &o = order[g * 32 + l];
+                if (t < (int)o.size() && o[t] >= 0) used |= 1u << (o[t] % 32);
+            }
+            for (int l = 0; l < 32; ++l) {
+                const auto &o = order[g * 32 + l];
+                int i;
+                if (t < (int)o.size() && o[t] >= 0) {
+                    i = o[t];
+                } else {
+                    int b = 0;  // a zero word in a bank no real entry of this step uses
+                    while (used & (1u << b)) ++b;
+                    used |= 1u << b;
+                    i = N + ((b - N % 32) + 32) % 32;
+                }
+                idx[(((size_t)g * (Kp / 8) + t / 8) * 32 + l) * 8 + t % 8] = (uint16_t)i;
+            }
+        }
+    void *d_idx = nullptr, *d_w = nullptr;
+    CSP_CUDA(cudaMalloc(&d_idx, idx.size() * sizeof(uint16_t)));
+    owned.push_back(d_idx);
+    CSP_CUDA(cudaMalloc(&d_w, (size_t)N * sizeof(float)));
+    owned.push_back(d_w);
+    CSP_CUDA(cudaMemcpy(d_idx, idx.data(), idx.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    CSP_CUDA(cudaMemcpy(d_w, w.data(), (size_t)N * sizeof(float), cudaMemcpyHostToDevice));
+    nd.l0_idx = (const uint4 *)d_idx;
+    nd.l0_w = (const float *)d_w;
+    nd.l0_k = Kp;
+    return 0;
+}
+
+int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms, int max_n) {
+    using F = void (*)(const NetDev *, int, int, unsigned long long *);
+    static const F fns[3] = {k_layer0_bits<float>, k_layer0_bits<__half>, k_layer0_bits<__nv_bfloat16>};
+    k.fn = (void *)fns[prec];
+    k.smem = (size_t)(max_n + 32) * 4;
+    CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+    k.grid = dim3(2 * sms);
+    k.block = dim3(kBitsThreads);
+    k.arg(nets).arg(nnets).arg(prec).arg(launches);
+    return COSPDNN_OK;
+}
+
+void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *bits, cudaStream_t s) {
+    const int64_t warps = (int64_t)((rows + 31) / 32) * (N / 32);
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warps + 7) / 8, 148 * 16));
+    if (format == COSPDNN_INPUT_BITS) k_convert_bits<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, rows, N, bits);
+    else k_convert_bits<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, rows, N, bits);
+}
+
+}  // namespace cospdnn

@@ -1,0 +1,25 @@
+// Layer 0 of binary inputs by bit counting (implementation in bits_layer.cu).
+#pragma once
+
+#include <vector>
+
+#include "engine.cuh"
+
+namespace cospdnn {
+
+// Builds the bit-count schedule of layer 0 of a row-tile net when every
+// output's weights are one value (zero entries ignored) and no output has
+// more than 63 of them; returns the steps per output (a multiple of 8), or 0
+// when the layer does not qualify (nothing is uploaded then).
+int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
+             int N, int prec, int TR, NetDev &nd, std::vector<void *> &owned);
+// Launch of the bit-count kernel for the qualifying nets of precision `prec`.
+int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms, int max_n);
+// Input rows (U8 or packed bits, row-major) as bit planes: word (unit, f)
+// holds feature f of rows 32*unit .. 32*unit+31 (bit r = row 32*unit+r is
+// non-zero; rows past `rows` are 0).
+void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *bits, cudaStream_t s);
+// Bytes of the bit planes of `rows` rows of width N.
+inline size_t l0_bits_bytes(int rows, int N) { return (size_t)((rows + 31) / 32) * N * 4; }
+
+}  // namespace cospdnn

@@ -170,7 +170,7 @@ __host__ __device__ __forceinline__ int cc_lane_bytes_of(int prec, int TR) {
 
 __device__ __forceinline__ bool cc_net(const NetDev &nd, int prec, int lb) {
     return nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 2 && nd.prec == prec && !nd.st->done &&
-           cc_lane_bytes_of(nd.prec, nd.layout) == lb;
+           cc_lane_bytes_of(nd.prec, nd.layout) == lb && !(nd.st->layer == 0 && nd.st->l0_bits);
 }
 
 // Output slices per tile: the split (1, 2, 4, ... up to one CTA round of
@@ -419,6 +419,8 @@ uint32_t weight_bits<__nv_bfloat16>(float w) {
     return (uint32_t)*reinterpret_cast<const uint16_t *>(&h);
 }
 
+}  // namespace
+
 // Edge colouring of one group's bipartite multigraph (P outputs x P
 // residues): colour[e] in [0, D), D = max degree, no two edges of a colour
 // share a vertex.  Alternating-path recolouring (König's constructive proof).
@@ -469,7 +471,6 @@ int colour_group(int P, const std::vector<int> &eu, const std::vector<int> &es, 
     return D;
 }
 
-}  // namespace
 
 int cc_tile_rows(int N, int prec) {
     const int es = prec == COSPDNN_PREC_FP32 ? 4 : 2;

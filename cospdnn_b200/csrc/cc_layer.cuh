@@ -21,6 +21,10 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
 // column; max_tile_bytes = largest N*TR*element size among them.
 int cc_layer_spec(KSpec &spec, NetDev *nets, int nnets, int prec, int lane_bytes, unsigned long long *launches,
                   int sms, size_t max_tile_bytes);
+// Edge colouring of a bipartite multigraph with P vertices on each side
+// (edge e joins eu[e] and es[e]): colour[e] in [0, D), D = the max degree, no
+// two edges of one colour share a vertex.  Returns D.
+int colour_group(int P, const std::vector<int> &eu, const std::vector<int> &es, std::vector<int> &colour);
 // Lane bytes of a row-tile net of tile height TR.
 inline int cc_lane_bytes(int prec, int TR) { return TR * (prec == COSPDNN_PREC_FP32 ? 4 : 2) >= 16 ? 16 : 8; }
 // Bytes of one row tile.

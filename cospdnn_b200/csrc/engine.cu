@@ -7,6 +7,7 @@
 #include <memory>
 #include <vector>
 
+#include "bits_layer.cuh"
 #include "cc_layer.cuh"
 #include "engine_kernels.cuh"
 #include "tc_layer.cuh"
@@ -175,9 +176,10 @@ __global__ void __launch_bounds__(256) k_convert_mma(const uint8_t *__restrict__
 }
 
 // Per-row max |input| (error 0) of integer inputs: one warp per row.
+// `nonbin` (may be NULL) is raised when a value is above 1.
 template <int FMT>
 __global__ void k_row_max(const uint8_t *__restrict__ src, int rows, int N, float *__restrict__ err0,
-                          float *__restrict__ mx0) {
+                          float *__restrict__ mx0, int *__restrict__ nonbin) {
     const int lane = threadIdx.x & 31;
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -201,6 +203,7 @@ __global__ void k_row_max(const uint8_t *__restrict__ src, int rows, int N, floa
         if (lane == 0) {
             err0[r] = 0.0f;
             mx0[r] = (float)m;
+            if (nonbin && m > 1u) atomicOr(nonbin, 1);
         }
     }
 }
@@ -257,6 +260,8 @@ struct Net {
     float *err0buf[2] = {nullptr, nullptr}, *mx0buf[2] = {nullptr, nullptr};
     float *f32buf[2] = {nullptr, nullptr};  // exact rows of FP32 inputs (allocated on first use)
     bool f32used[2] = {false, false};       // the buffer's last input came as FP32
+    uint32_t *bitsbuf[2] = {nullptr, nullptr};  // bit planes of binary inputs (layer 0 by counting)
+    int *nbflag[2] = {nullptr, nullptr};        // raised when that input is not binary
     int front = 0;                          // buffers of the current input
     bool pending = false;                   // the back buffers hold a newer input
 };
@@ -297,6 +302,7 @@ struct cospdnn_engine {
     cudaGraphConditionalHandle loop{};
     KSpec k0, k2, k3, k4_graph, k4_eager, k5;
     std::vector<KSpec> layer_specs;
+    std::vector<KSpec> l0_specs;  // layer 0 by bit counting, once per run before the layer loop
     std::vector<long long *> packbuf;  // per net: device buffer for result_async
     ~cospdnn_engine() {
         int cur = 0;
@@ -440,6 +446,16 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
+    for (int prec = 0; prec < 3; ++prec) {
+        int max_n = 0;
+        for (const Net &n : e->nets)
+            if (n.dev.l0_k > 0 && n.d.precision == prec) max_n = std::max(max_n, n.d.neuron);
+        if (!max_n) continue;
+        KSpec k;
+        int rc = l0_spec(k, nets, nn, prec, launches, sms, max_n);
+        if (rc) return rc;
+        e->l0_specs.push_back(std::move(k));
+    }
     for (int prec : ks.tc) {
         KSpec k;
         int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, sms);
@@ -497,6 +513,9 @@ int build_graph(cospdnn_engine *e, const KernelSets &ks) {
     if (rc) return rc;
     cudaGraphNode_t k0;
     if ((rc = add_node(e->graph, &k0, nullptr, 0, e->k0))) return rc;
+    std::vector<cudaGraphNode_t> l0_nodes(e->l0_specs.size());
+    for (size_t i = 0; i < e->l0_specs.size(); ++i)
+        if ((rc = add_node(e->graph, &l0_nodes[i], &k0, 1, e->l0_specs[i]))) return rc;
     // while (any network live) { layer kernels; classify; FP64 replay; compact }
     cudaGraphNodeParams cp{};
     cp.type = cudaGraphNodeTypeConditional;
@@ -504,7 +523,8 @@ int build_graph(cospdnn_engine *e, const KernelSets &ks) {
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t cnode;
-    CSP_CUDA(cudaGraphAddNode(&cnode, e->graph, &k0, 1, &cp));
+    if (l0_nodes.empty()) CSP_CUDA(cudaGraphAddNode(&cnode, e->graph, &k0, 1, &cp));
+    else CSP_CUDA(cudaGraphAddNode(&cnode, e->graph, l0_nodes.data(), l0_nodes.size(), &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     std::vector<cudaGraphNode_t> layer_nodes(e->layer_specs.size());
     for (size_t i = 0; i < e->layer_specs.size(); ++i)
@@ -668,6 +688,22 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     for (Net &n : e->nets) {
         const int N = n.d.neuron, R = std::max(1, n.d.rows);
         n.ldev.resize(n.d.layers);
+        if (n.dev.kernel == COSPDNN_KERNEL_CUDA_CORE && n.dev.layout >= 4 && n.d.layers > 0) {
+            const HostLayer &h0 = n.layers[0];
+            int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, n.dev.layout, n.dev, e->owned);
+            if (rc) return rc;
+            if (n.dev.l0_k > 0) {
+                for (int b = 0; b < 2; ++b) {
+                    n.bitsbuf[b] = dalloc<uint32_t>(l0_bits_bytes(R, N) / 4, e->owned);
+                    n.nbflag[b] = dalloc<int>(1, e->owned);
+                    CSP_CHECK(n.bitsbuf[b] && n.nbflag[b], COSPDNN_ERR_NOMEM, "build: device allocation failed");
+                    CSP_CUDA(cudaMemset(n.bitsbuf[b], 0, l0_bits_bytes(R, N)));
+                    CSP_CUDA(cudaMemset(n.nbflag[b], 1, sizeof(int)));  // no input yet
+                }
+                n.dev.y0bits = n.bitsbuf[0];
+                n.dev.y0nonbin = n.nbflag[0];
+            }
+        }
         for (int l = 0; l < n.d.layers; ++l) {
             int rc = upload_layer(e, n, l, n.ldev[l]);
             if (rc) return rc;
@@ -824,10 +860,15 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
         else if (n.d.precision == COSPDNN_PREC_FP16) CSP_PIECES(__half);
         else CSP_PIECES(__nv_bfloat16);
 #undef CSP_PIECES
-        if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
-        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
+        if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
+        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
         CSP_CUDA(cudaGetLastError());
         return COSPDNN_OK;
+    }
+    if (n.nbflag[back]) {
+        // binary unless the row maxima say otherwise (FP32 values: never counted)
+        CSP_CUDA(cudaMemsetAsync(n.nbflag[back], format == COSPDNN_INPUT_F32 ? 1 : 0, sizeof(int), s));
+        if (format != COSPDNN_INPUT_F32) l0_convert_bits((const uint8_t *)src, format, R, N, n.bitsbuf[back], s);
     }
     if (n.dev.layout >= 2 && format != COSPDNN_INPUT_F32) {
         // integer input into row tiles
@@ -840,8 +881,9 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
         else if (n.d.precision == COSPDNN_PREC_FP16) CSP_TILE(__half);
         else CSP_TILE(__nv_bfloat16);
 #undef CSP_TILE
-        if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
-        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0);
+        if (format == COSPDNN_INPUT_U8)
+            k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, n.nbflag[back]);
+        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
         CSP_CUDA(cudaGetLastError());
         return COSPDNN_OK;
     }
@@ -875,6 +917,10 @@ int take_inputs(cospdnn_engine *e, cudaStream_t s) {
         n.dev.err0 = n.err0buf[n.front];
         n.dev.mx0 = n.mx0buf[n.front];
         n.dev.y0_f32 = n.f32used[n.front] ? n.f32buf[n.front] : nullptr;
+        if (n.bitsbuf[n.front]) {
+            n.dev.y0bits = n.bitsbuf[n.front];
+            n.dev.y0nonbin = n.nbflag[n.front];
+        }
         // from pageable memory: the descriptor is staged before the call returns
         CSP_CUDA(cudaMemcpyAsync(e->d_nets + i, &n.dev, sizeof(NetDev), cudaMemcpyHostToDevice, s));
     }
@@ -1035,6 +1081,8 @@ extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, in
         for (auto &x : st) live |= !x.done;
         if (!live) break;
         cudaEventRecord(a, s);
+        if (it == 0)
+            for (KSpec &k : e->l0_specs) if (!rc) rc = launch(k, s);
         for (KSpec &k : e->layer_specs) if (!rc) rc = launch(k, s);
         cudaEventRecord(b, s);
         if (!rc) rc = launch(e->k2, s);

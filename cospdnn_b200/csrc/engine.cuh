@@ -77,7 +77,7 @@ struct NetState {
     int err;     // device-side error code (0 = ok)
     int in_buf;  // act[in_buf] is the input of `layer` (layer 0 reads y0)
     int copy_R;  // rows the pending compaction copies (0 = none pending)
-    int pad;
+    int l0_bits; // layer 0 of this run was computed by the bit-count kernel
 };
 
 struct NetDev {
@@ -102,6 +102,15 @@ struct NetDev {
     long long *alive_count;  // [L] rows kept after layer l
     long long *recheck_count;// [L] rows re-decided in FP64 at layer l
     NetState *st;
+    // layer 0 by bit counting (bits_layer.cu): binary inputs as bit planes
+    // [(rows+31)/32][N] words, a flag raised when the current input is not
+    // binary, and the schedule of layer 0 (l0_k steps per output, 0 = the
+    // layer does not qualify: not one weight value per output)
+    const uint32_t *y0bits;
+    const int *y0nonbin;
+    const uint4 *l0_idx;     // [N/32][l0_k/8][32] x 8 input indices (16 bits)
+    const float *l0_w;       // [N] the output's weight in the compute type
+    int l0_k;
 };
 
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };

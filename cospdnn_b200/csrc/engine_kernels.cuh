@@ -37,6 +37,7 @@ __global__ void k_init_run(const NetDev *__restrict__ nets, int nnets, unsigned 
             nd.st->err = 0;
             nd.st->in_buf = 0;
             nd.st->copy_R = 0;
+            nd.st->l0_bits = 0;
         }
         for (int64_t l = tid; l < nd.L; l += nth) {
             nd.alive_count[l] = 0;

@@ -318,3 +318,60 @@ def test_engine_next_input_set_during_run(cs):
     eng.close()
     for r, ref in zip(got, [ref_a, ref_b, ref_a, ref_b]):
         check_parity(r, ref, L)
+
+
+@pytest.mark.parametrize("n,prec,rows", [(1024, 1, 333), (4096, 1, 5), (16384, 2, 97), (1024, 0, 333),
+                                         (2048, 0, 64), (512, 1, 333)])
+def test_layer0_bit_count_matches_general_kernel(cs, n, prec, rows):
+    """Layer 0 by bit counting (binary inputs, one weight value per output)
+    stores exactly what the general row-tile kernel stores: a one-layer net
+    run on U8 and packed-bit inputs (counted) and on the same rows as FP32
+    (never counted); row tiles of 64, 32, 16, 8 and 4 rows.  Per-output
+    weight values differ (1/16 times 1, 2 or 3), so the kernel reads each
+    output's own weight."""
+    from oracle import pyoracle as po
+    cp, ri, vv = po.masks_to_csc(po.xor_masks(59, 0, 0, n), n)
+    col = np.repeat(np.arange(n), np.diff(cp))
+    vv = (vv * (1 + col % 3)).astype(np.float32)
+    y0 = po.input_binary(59, 0, rows, n, 0.1, 0.3)
+    b = np.float32(-0.3)
+    ref = oracle_run([(cp, ri, vv)], y0, b)
+    eng = cs.Engine(0)
+    nid = eng.add_net(n, 1, rows, float(b), 1e-5, prec, 1)
+    eng.set_layer_csc(nid, 0, cp, ri, vv)
+    eng.build()
+    outs = []
+    bits = np.packbits(y0, axis=1, bitorder="little")
+    for x, fmt in ((y0, cs.INPUT_U8), (bits, cs.INPUT_BITS), (y0.astype(np.float32), cs.INPUT_F32)):
+        eng.set_input(nid, x, fmt=fmt)
+        eng.run()
+        r = eng.result(nid)
+        check_parity(r, ref, 1)
+        outs.append(eng.final_values(nid, len(r["categories"])))
+    eng.close()
+    np.testing.assert_array_equal(outs[0], outs[2])
+    np.testing.assert_array_equal(outs[1], outs[2])
+
+
+def test_layer0_bit_count_falls_back(cs):
+    """Inputs with a value above 1, and layers whose outputs mix weight
+    values, take the general kernel; results stay exact."""
+    from netgen import random_layer
+    from oracle import pyoracle as po
+    n, rows = 1024, 200
+    xor = po.masks_to_csc(po.xor_masks(61, 0, 0, n), n)
+    mixed = random_layer(n, 61, 0)
+    y0 = po.input_binary(61, 0, rows, n, 0.1, 0.3)
+    y2 = y0.copy()
+    y2[::7] *= 2  # values 0 and 2 in every seventh row
+    for layer, x in ((xor, y2), (mixed, y0)):
+        ref = oracle_run([layer, xor], x, np.float32(-0.3))
+        eng = cs.Engine(0)
+        nid = eng.add_net(n, 2, rows, -0.3, 1e-5, 1, 1)
+        eng.set_layer_csc(nid, 0, *layer)
+        eng.set_layer_csc(nid, 1, *xor)
+        eng.build()
+        eng.set_input(nid, x)
+        eng.run()
+        check_parity(eng.result(nid), ref, 2)
+        eng.close()
