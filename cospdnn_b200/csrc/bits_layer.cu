@@ -10,8 +10,8 @@
 // Harley-Seal: about 2.4 logic instructions per word for 32 rows).  The
 // counts are moved into bytes four rows at a time (a multiply spreads 4 bits
 // of a plane into 4 bytes), then bias, clamp and the store in the compute
-// type follow the row-tile kernel's epilogue, with the same per-row
-// statistics for the keep/prune decision.  Shared-memory traffic per output
+// type follow the row-tile kernel's epilogue, with its per-row statistics
+// for the keep/prune decision (the output error bound kept for every row).  Shared-memory traffic per output
 // and 32 rows is 32 words against 32 * 32 rows of 16-bit values in the
 // general kernel.
 //
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
     count_launch(launches);
     extern __shared__ uint4 l0_smem[];
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(l0_smem);
-    __shared__ uint32_t s_zmax[32], s_zdist[32];
+    __shared__ uint32_t s_zmax[32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
@@ -115,16 +115,12 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                 if (threadIdx.x < 32) {
                     s_bits[N + threadIdx.x] = 0u;  // padding words, one per bank
                     s_zmax[threadIdx.x] = 0u;
-                    s_zdist[threadIdx.x] = 0x7F800000u;
                 }
             }
             __syncthreads();
-            float zmx[32], zds[32];
+            float zmx[32];
 #pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                zmx[r] = -INFINITY;
-                zds[r] = INFINITY;
-            }
+            for (int r = 0; r < 32; ++r) zmx[r] = -INFINITY;
             for (int g = warp; g < ngroups; g += kBitsWarps) {
                 const int j = g * 32 + lane;
                 uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
@@ -146,9 +142,10 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int r = 4 * q + k;
-                        const float z = fmaf((float)((c4 >> (8 * k)) & 0xFFu), w, bias);
+                        // byte k of c4 as the mantissa of 2^23 + count: exact, no conversion
+                        const float cnt = __uint_as_float(__byte_perm(c4, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
+                        const float z = fmaf(cnt, w, bias);
                         zmx[r] = fmaxf(zmx[r], z);
-                        zds[r] = fminf(zds[r], fabsf(z - 16.0f));
                         ov[r] = act_traits<T>::from_f(clamp32(z));
                     }
                 }
@@ -166,15 +163,11 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                     }
                 }
             }
-            // row statistics: over the warp's outputs, then over the CTA
+            // row max over the warp's outputs, then over the CTA
 #pragma unroll
             for (int r = 0; r < 32; ++r) {
                 const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
-                const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
-                if (lane == r) {
-                    atomicMax(&s_zmax[r], m);
-                    atomicMin(&s_zdist[r], d);
-                }
+                if (lane == r) atomicMax(&s_zmax[r], m);
             }
             __syncthreads();
             if (threadIdx.x < 32) {
@@ -182,19 +175,18 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                 if (p < R) {
                     const double steps = fast_steps(nd, lw);
                     const float ez = z_error_bound(nd.err[0][p], nd.mx[0][p], lw.S, lw.dW, bias, steps);
-                    float em, ym;
                     const float zm = ord2f(s_zmax[threadIdx.x]);
-                    const float zd = __uint_as_float(s_zdist[threadIdx.x]);
                     const float c = clamp32(zm);
-                    ym = act_traits<T>::to_f(act_traits<T>::from_f(c));
-                    // as the row-tile kernel (row_stats): outputs within 16 + ez of 16
-                    // carry the bound plus their storage rounding
+                    const float ym = act_traits<T>::to_f(act_traits<T>::from_f(c));
+                    // output error: the bound plus the storage rounding of the row's
+                    // largest output (the row-tile kernel also drops it when every
+                    // output is exactly 0 or 32; keeping it is never smaller)
                     float se = 0.0f;
                     if constexpr (sizeof(T) == 2) {
                         se = std::is_same<T, __half>::value ? __fmaf_ru(c, 4.8828125e-04f, 2.98023224e-08f)
                                                             : __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
                     }
-                    em = zd < 16.0f + ez ? __fadd_ru(ez, se) : 0.0f;
+                    const float em = __fadd_ru(ez, se);
                     atomicMax(&nd.stat[3 * p], s_zmax[threadIdx.x]);
                     atomicMax(&nd.stat[3 * p + 1], __float_as_uint(em));
                     atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));
