@@ -196,44 +196,70 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
     }
 }
 
-// Bit planes of U8 (FMT 0) or packed-bit (FMT 2) rows: one warp per
-// (unit of 32 rows, 32 features); lane r reads row 32*unit + r.
+// A 32x32 bit matrix held one row per lane (bit k of lane r = element (r, k))
+// transposed in place: afterwards bit r of lane k = the old element (r, k).
+// Five rounds swap the off-diagonal blocks of size j between lanes r and r^j.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint32_t m = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu
+                         : j == 2 ? 0x33333333u : 0x55555555u;  // bits k with (k & j) == 0
+        const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+        if (lane & j) x = (x & ~m) | ((y >> j) & m);
+        else x = (x & m) | ((y << j) & ~m);
+    }
+    return x;
+}
+
+// Bit planes of U8 (FMT 0) or packed-bit (FMT 2) rows, with the row maxima
+// (error 0) and, for bytes, the flag raised by a value above 1: one warp per
+// unit of 32 rows, lane r reading row 32*unit + r 32 features at a time and
+// the warp transposing each 32x32 block (coalesced 128-byte stores).
 template <int FMT>
-__global__ void k_convert_bits(const uint8_t *__restrict__ src, int rows, int N, uint32_t *__restrict__ bits) {
+__global__ void k_convert_bits(const uint8_t *__restrict__ src, int rows, int N, uint32_t *__restrict__ bits,
+                               float *__restrict__ err0, float *__restrict__ mx0, int *__restrict__ nonbin) {
     const int lane = threadIdx.x & 31;
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int units = (rows + 31) / 32, fgroups = N / 32;
-    for (int64_t t = w; t < (int64_t)units * fgroups; t += nw) {
-        const int u = (int)(t / fgroups), fg = (int)(t % fgroups);
-        const int64_t row = (int64_t)u * 32 + lane;
-        uint32_t mine = 0;  // bit k = feature 32*fg + k of this lane's row
-        if (row < rows) {
-            if (FMT == COSPDNN_INPUT_BITS) {
-                const uint8_t *b = src + row * (N / 8) + fg * 4;
-                mine = (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
-            } else {
-                const uint8_t *b = src + row * N + fg * 32;
+    const int units = (rows + 31) / 32, nfb = N / 32;
+    for (int64_t u = w; u < units; u += nw) {
+        const int64_t row = u * 32 + lane;
+        const bool valid = row < rows;
+        uint32_t rmax = 0;
+        for (int fb = 0; fb < nfb; ++fb) {
+            uint32_t x = 0;  // bit k = feature 32*fb + k of this lane's row
+            if (valid) {
+                if (FMT == COSPDNN_INPUT_BITS) {
+                    const uint8_t *b = src + row * (N / 8) + fb * 4;  // rows of N/8 bytes: any alignment
+                    x = (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+                    rmax |= x;
+                } else {
+                    const uint8_t *b = src + row * N + fb * 32;
 #pragma unroll
-                for (int k = 0; k < 32; k += 8) {
-                    const uint2 v = *reinterpret_cast<const uint2 *>(b + k);  // N % 32 == 0: 8-byte aligned
-                    const uint32_t lo = v.x, hi = v.y;
+                    for (int k = 0; k < 32; k += 8) {
+                        const uint2 v = *reinterpret_cast<const uint2 *>(b + k);  // N % 32 == 0: 8-byte aligned
+                        rmax = max(rmax, __vmaxu4(v.x, v.y));
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        mine |= (((lo >> (8 * i)) & 0xFFu) ? 1u : 0u) << (k + i);
-                        mine |= (((hi >> (8 * i)) & 0xFFu) ? 1u : 0u) << (k + 4 + i);
+                        for (int i = 0; i < 4; ++i) {
+                            x |= (((v.x >> (8 * i)) & 0xFFu) ? 1u : 0u) << (k + i);
+                            x |= (((v.y >> (8 * i)) & 0xFFu) ? 1u : 0u) << (k + 4 + i);
+                        }
                     }
                 }
             }
+            bits[u * N + fb * 32 + lane] = transpose32(x, lane);
         }
-        // transpose: feature k's word has bit lane set when this lane's row has it
-        uint32_t outw = 0;
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-            const uint32_t bal = __ballot_sync(0xffffffffu, (mine >> k) & 1u);
-            if (lane == k) outw = bal;
+        if (valid) {
+            uint32_t m;
+            if (FMT == COSPDNN_INPUT_BITS) {
+                m = rmax ? 1u : 0u;
+            } else {
+                m = max(max(rmax & 0xFFu, (rmax >> 8) & 0xFFu), max((rmax >> 16) & 0xFFu, rmax >> 24));
+                if (m > 1u) atomicOr(nonbin, 1);
+            }
+            err0[row] = 0.0f;
+            mx0[row] = (float)m;
         }
-        bits[(int64_t)u * N + fg * 32 + lane] = outw;
     }
 }
 
@@ -337,11 +363,13 @@ int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *lau
     return COSPDNN_OK;
 }
 
-void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *bits, cudaStream_t s) {
-    const int64_t warps = (int64_t)((rows + 31) / 32) * (N / 32);
+void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *bits, float *err0, float *mx0,
+                     int *nonbin, cudaStream_t s) {
+    const int64_t warps = (rows + 31) / 32;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warps + 7) / 8, 148 * 16));
-    if (format == COSPDNN_INPUT_BITS) k_convert_bits<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, rows, N, bits);
-    else k_convert_bits<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, rows, N, bits);
+    if (format == COSPDNN_INPUT_BITS)
+        k_convert_bits<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, rows, N, bits, err0, mx0, nonbin);
+    else k_convert_bits<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, rows, N, bits, err0, mx0, nonbin);
 }
 
 }  // namespace cospdnn

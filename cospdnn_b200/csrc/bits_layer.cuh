@@ -17,8 +17,11 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
 int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms, int max_n);
 // Input rows (U8 or packed bits, row-major) as bit planes: word (unit, f)
 // holds feature f of rows 32*unit .. 32*unit+31 (bit r = row 32*unit+r is
-// non-zero; rows past `rows` are 0).
-void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *bits, cudaStream_t s);
+// non-zero; rows past `rows` are 0); also each row's max value (err0 = 0,
+// the row-max kernel's output) and, for bytes, `nonbin` raised when a value
+// is above 1 (the caller clears it first).
+void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *bits, float *err0, float *mx0,
+                     int *nonbin, cudaStream_t s);
 // Bytes of the bit planes of `rows` rows of width N.
 inline size_t l0_bits_bytes(int rows, int N) { return (size_t)((rows + 31) / 32) * N * 4; }
 

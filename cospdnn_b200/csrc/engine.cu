@@ -51,8 +51,13 @@ __global__ void k_convert_input(const void *__restrict__ src, int rows, int N, i
 // per (tile, run of up to 8 rows, 8 features); each feature's run of rows is
 // written as one contiguous piece.  Values 0..255 are exact in every compute
 // type, so the per-row error is 0 (k_row_max fills it and the row max).
+// `skip_if_binary` (may be NULL): the net counts layer 0 on bit planes when
+// the input is binary, and nothing reads this copy then, so the kernel
+// returns when the flag (raised by k_row_max for a value above 1) is clear.
 template <typename T, int FMT>
-__global__ void k_convert_tile(const uint8_t *__restrict__ src, int rows, int N, int TR, T *__restrict__ y0) {
+__global__ void k_convert_tile(const uint8_t *__restrict__ src, int rows, int N, int TR, T *__restrict__ y0,
+                               const int *__restrict__ skip_if_binary) {
+    if (skip_if_binary && *skip_if_binary == 0) return;
     const int RC = TR < 8 ? TR : 8, nrc = TR / RC, nfb = N / 8;
     const int64_t ntiles = (rows + TR - 1) / TR;
     const int64_t total = ntiles * nrc * nfb;
@@ -868,7 +873,6 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     if (n.nbflag[back]) {
         // binary unless the row maxima say otherwise (FP32 values: never counted)
         CSP_CUDA(cudaMemsetAsync(n.nbflag[back], format == COSPDNN_INPUT_F32 ? 1 : 0, sizeof(int), s));
-        if (format != COSPDNN_INPUT_F32) l0_convert_bits((const uint8_t *)src, format, R, N, n.bitsbuf[back], s);
     }
     if (n.dev.layout >= 2 && format != COSPDNN_INPUT_F32) {
         // integer input into row tiles
@@ -876,14 +880,29 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
         const int TR = n.dev.layout;
         const int64_t units = (int64_t)((R + TR - 1) / TR) * (TR / std::min(TR, 8)) * (N / 8);
         const int cb = (int)std::min<int64_t>((units + 255) / 256, 148 * 16);
-#define CSP_TILE(T)                                                                                             do {                                                                                                            if (format == COSPDNN_INPUT_U8) k_convert_tile<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)y0dst);         else k_convert_tile<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)y0dst);                } while (0)
-        if (n.d.precision == COSPDNN_PREC_FP32) CSP_TILE(float);
-        else if (n.d.precision == COSPDNN_PREC_FP16) CSP_TILE(__half);
-        else CSP_TILE(__nv_bfloat16);
-#undef CSP_TILE
-        if (format == COSPDNN_INPUT_U8)
-            k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, n.nbflag[back]);
+        // row maxima first: their binary flag decides whether the compute-type
+        // copy is needed (a net counting layer 0 reads the bit planes instead,
+        // and packed bits are always binary); for such a net the bit-plane
+        // conversion writes them
+        if (n.nbflag[back])
+            l0_convert_bits(b, format, R, N, n.bitsbuf[back], err0, mx0, n.nbflag[back], s);
+        else if (format == COSPDNN_INPUT_U8)
+            k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
         else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
+        const int *skip = n.nbflag[back];
+        if (!(skip && format == COSPDNN_INPUT_BITS)) {
+#define CSP_TILE(T)                                                                                             \
+    do {                                                                                                        \
+        if (format == COSPDNN_INPUT_U8)                                                                         \
+            k_convert_tile<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)y0dst, skip);             \
+        else                                                                                                    \
+            k_convert_tile<T, COSPDNN_INPUT_BITS><<<cb, 256, 0, s>>>(b, R, N, TR, (T *)y0dst, nullptr);        \
+    } while (0)
+            if (n.d.precision == COSPDNN_PREC_FP32) CSP_TILE(float);
+            else if (n.d.precision == COSPDNN_PREC_FP16) CSP_TILE(__half);
+            else CSP_TILE(__nv_bfloat16);
+#undef CSP_TILE
+        }
         CSP_CUDA(cudaGetLastError());
         return COSPDNN_OK;
     }

@@ -212,8 +212,13 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
     const int N = nd.N, l = nd.st->layer, par = l & 1, ib = nd.st->in_buf;
     const int orow = nd.orig[par][p];
     double *y = buf0, *z = buf1;
+    // the input row: exact FP32 values, the bit planes when layer 0 of this
+    // run was counted (the compute-type copy is not made then), else the
+    // compute-type copy (integer inputs are exact in it)
+    const bool counted = nd.st->l0_bits != 0;
     for (int j = threadIdx.x; j < N; j += blockDim.x)
         y[j] = nd.y0_f32 ? (double)nd.y0_f32[(int64_t)orow * N + j]
+             : counted   ? (double)((nd.y0bits[(int64_t)(orow >> 5) * N + j] >> (orow & 31)) & 1u)
                          : act_traits<T>::to_d(((const T *)nd.y0)[act_index(nd.layout, N, orow, j)]);
     __syncthreads();
     const double b = (double)nd.bias;
