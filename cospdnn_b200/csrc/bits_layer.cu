@@ -10,8 +10,9 @@
 // Harley-Seal: about 2.4 logic instructions per word for 32 rows).  The
 // counts are moved into bytes four rows at a time (a multiply spreads 4 bits
 // of a plane into 4 bytes), then bias, clamp and the store in the compute
-// type follow the row-tile kernel's epilogue, with its per-row statistics
-// for the keep/prune decision (the output error bound kept for every row).  Shared-memory traffic per output
+// type follow the epilogue of the kernel the net uses otherwise, with its
+// per-row statistics for the keep/prune decision, so the stored values and
+// the rows sent to the FP64 recheck are the same as without counting.  Shared-memory traffic per output
 // and 32 rows is 32 words against 32 * 32 rows of 16-bit values in the
 // general kernel.
 //
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
     count_launch(launches);
     extern __shared__ uint4 l0_smem[];
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(l0_smem);
-    __shared__ uint32_t s_zmax[32];
+    __shared__ uint32_t s_zmax[32], s_zdist[32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
@@ -115,12 +116,16 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                 if (threadIdx.x < 32) {
                     s_bits[N + threadIdx.x] = 0u;  // padding words, one per bank
                     s_zmax[threadIdx.x] = 0u;
+                    s_zdist[threadIdx.x] = 0x7F800000u;
                 }
             }
             __syncthreads();
-            float zmx[32];
+            float zmx[32], zds[32];
 #pragma unroll
-            for (int r = 0; r < 32; ++r) zmx[r] = -INFINITY;
+            for (int r = 0; r < 32; ++r) {
+                zmx[r] = -INFINITY;
+                zds[r] = INFINITY;
+            }
             for (int g = warp; g < ngroups; g += kBitsWarps) {
                 const int j = g * 32 + lane;
                 uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
@@ -146,6 +151,7 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                         const float cnt = __uint_as_float(__byte_perm(c4, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
                         const float z = fmaf(cnt, w, bias);
                         zmx[r] = fmaxf(zmx[r], z);
+                        zds[r] = fminf(zds[r], fabsf(z - 16.0f));
                         ov[r] = act_traits<T>::from_f(clamp32(z));
                     }
                 }
@@ -163,11 +169,15 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                     }
                 }
             }
-            // row max over the warp's outputs, then over the CTA
+            // row max z and min |z - 16| over the warp's outputs, then over the CTA
 #pragma unroll
             for (int r = 0; r < 32; ++r) {
                 const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
-                if (lane == r) atomicMax(&s_zmax[r], m);
+                const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
+                if (lane == r) {
+                    atomicMax(&s_zmax[r], m);
+                    atomicMin(&s_zdist[r], d);
+                }
             }
             __syncthreads();
             if (threadIdx.x < 32) {
@@ -175,20 +185,138 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                 if (p < R) {
                     const double steps = fast_steps(nd, lw);
                     const float ez = z_error_bound(nd.err[0][p], nd.mx[0][p], lw.S, lw.dW, bias, steps);
+                    // the row-tile kernel's statistics (row_stats): max output, and the
+                    // bound plus the storage rounding when some output is within
+                    // 16 + ez of 16
                     const float zm = ord2f(s_zmax[threadIdx.x]);
+                    const float zd = __uint_as_float(s_zdist[threadIdx.x]);
                     const float c = clamp32(zm);
                     const float ym = act_traits<T>::to_f(act_traits<T>::from_f(c));
-                    // output error: the bound plus the storage rounding of the row's
-                    // largest output (the row-tile kernel also drops it when every
-                    // output is exactly 0 or 32; keeping it is never smaller)
                     float se = 0.0f;
                     if constexpr (sizeof(T) == 2) {
                         se = std::is_same<T, __half>::value ? __fmaf_ru(c, 4.8828125e-04f, 2.98023224e-08f)
                                                             : __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
                     }
-                    const float em = __fadd_ru(ez, se);
+                    const float em = zd < 16.0f + ez ? __fadd_ru(ez, se) : 0.0f;
                     atomicMax(&nd.stat[3 * p], s_zmax[threadIdx.x]);
                     atomicMax(&nd.stat[3 * p + 1], __float_as_uint(em));
+                    atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));
+                }
+            }
+        }
+    }
+}
+
+// MMA-tile (tcgen05) nets: units of 16 rows, so that the words of a unit
+// (16 bits per feature) fit in shared memory up to 65536 features; a lane
+// packs two entries' 16-bit words into one 32-bit word (the even entry in
+// the low half), counts them as above and adds the two halves' counts; each
+// output value is stored into its MMA operand tile (act_index layout 1).
+constexpr int kBits16Threads = 512;
+constexpr int kBits16Warps = kBits16Threads / 32;
+
+__device__ __forceinline__ bool l0_net16(const NetDev &nd, int prec) {
+    return nd.l0_k > 0 && nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.layout == 1 && nd.prec == prec &&
+           !nd.st->done && nd.st->layer == 0 && nd.y0bits != nullptr && *nd.y0nonbin == 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBits16Threads, 1)
+    k_layer0_bits16(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
+    count_launch(launches);
+    extern __shared__ uint4 l0_smem[];
+    uint16_t *s_w = reinterpret_cast<uint16_t *>(l0_smem);
+    __shared__ uint32_t s_zmax[16], s_emax[16];
+    __shared__ float s_ez[16];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int n = 0; n < nnets; ++n) {
+        const NetDev &nd = nets[n];
+        if (!l0_net16(nd, prec)) continue;
+        if (blockIdx.x == 0 && threadIdx.x == 0) nd.st->l0_bits = 1;  // the tcgen05 kernel skips layer 0
+        const int N = nd.N, R = nd.st->R, K4 = nd.l0_k / 4;
+        const int units = (R + 15) / 16, ngroups = N / 32;
+        const LayerDev &lw = nd.layers[0];
+        T *out = (T *)nd.act[nd.st->in_buf ^ 1];
+        const float bias = nd.bias;
+        for (int u = blockIdx.x; u < units; u += gridDim.x) {
+            __syncthreads();  // the previous unit is done with the words and the row maxima
+            {
+                // half (u & 1) of the 32-row words of unit u / 2
+                const int sh = (u & 1) * 16;
+                const uint4 *src = reinterpret_cast<const uint4 *>(nd.y0bits + (int64_t)(u >> 1) * N);
+                for (int i = threadIdx.x; i < N / 4; i += kBits16Threads) {
+                    const uint4 v = __ldg(src + i);
+                    reinterpret_cast<uint2 *>(s_w)[i] =
+                        make_uint2(((v.x >> sh) & 0xFFFFu) | (((v.y >> sh) & 0xFFFFu) << 16),
+                                   ((v.z >> sh) & 0xFFFFu) | (((v.w >> sh) & 0xFFFFu) << 16));
+                }
+                if (threadIdx.x < 32) reinterpret_cast<uint32_t *>(s_w + N)[threadIdx.x] = 0u;  // padding
+                if (threadIdx.x < 16) {
+                    const int p = min(u * 16 + (int)threadIdx.x, R - 1);
+                    s_zmax[threadIdx.x] = 0u;
+                    s_emax[threadIdx.x] = 0u;
+                    s_ez[threadIdx.x] =
+                        z_error_bound(nd.err[0][p], nd.mx[0][p], lw.S, lw.dW, bias, fast_steps(nd, lw));
+                }
+            }
+            __syncthreads();
+            float zmx[16], ems[16], ezr[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                zmx[r] = -INFINITY;
+                ems[r] = 0.0f;
+                ezr[r] = s_ez[r];
+            }
+            for (int g = warp; g < ngroups; g += kBits16Warps) {
+                const int j = g * 32 + lane;
+                uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+                const uint4 *ent = nd.l0_idx + (int64_t)g * K4 * 32 + lane;
+                for (int t = 0; t < K4; t += 4) {  // 16 entries, 8 packed words
+                    uint32_t x[8];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const uint4 q = __ldg(ent + (int64_t)(t + v) * 32);
+                        x[2 * v] = (uint32_t)s_w[q.x] | ((uint32_t)s_w[q.y] << 16);
+                        x[2 * v + 1] = (uint32_t)s_w[q.z] | ((uint32_t)s_w[q.w] << 16);
+                    }
+                    add8(p, x);
+                }
+                const float w = nd.l0_w[j];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t c4 = counts4(p, q) + counts4(p, q + 4);  // even + odd entries (each <= 32)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int r = 4 * q + k;
+                        const float cnt = __uint_as_float(__byte_perm(c4, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
+                        const float z = fmaf(cnt, w, bias);
+                        const float cz = clamp32(z);
+                        const T o = act_traits<T>::from_f(cz);
+                        zmx[r] = fmaxf(zmx[r], z);
+                        // the tcgen05 epilogue's error of an output near the clamp range
+                        if (z > -ezr[r] && z < 32.0f + ezr[r])
+                            ems[r] = fmaxf(ems[r], __fadd_ru(ezr[r], fabsf(act_traits<T>::to_f(o) - cz)));
+                        out[act_index(1, N, (int64_t)u * 16 + r, j)] = o;
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
+                const uint32_t e = __reduce_max_sync(0xffffffffu, __float_as_uint(ems[r]));  // >= 0
+                if (lane == r) {
+                    atomicMax(&s_zmax[r], m);
+                    atomicMax(&s_emax[r], e);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < 16) {
+                const int p = u * 16 + threadIdx.x;
+                if (p < R) {
+                    const float c = clamp32(ord2f(s_zmax[threadIdx.x]));
+                    const float ym = act_traits<T>::to_f(act_traits<T>::from_f(c));  // the max stored output
+                    atomicMax(&nd.stat[3 * p], s_zmax[threadIdx.x]);
+                    atomicMax(&nd.stat[3 * p + 1], s_emax[threadIdx.x]);
                     atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));
                 }
             }
@@ -266,11 +394,14 @@ __global__ void k_convert_bits(const uint8_t *__restrict__ src, int rows, int N,
 }  // namespace
 
 int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
-             int N, int prec, int TR, NetDev &nd, std::vector<void *> &owned) {
+             int N, int prec, int layout, NetDev &nd, std::vector<void *> &owned) {
     nd.l0_k = 0;
     nd.l0_idx = nullptr;
     nd.l0_w = nullptr;
-    if (TR < 4 || N % 32 != 0 || N + 32 > 65535) return 0;
+    // row-tile nets: 32-bit words (32 rows), 16-bit indices, steps in 8s;
+    // MMA-tile nets: 16-bit words (16 rows), 32-bit indices, steps in 16s
+    const bool half = layout == 1;
+    if (N % 32 != 0 || (!half && (layout < 4 || N + 32 > 65535))) return 0;
     // one weight value per output, at most 63 non-zero entries
     std::vector<float> w(N, 0.0f);
     std::vector<std::vector<int>> ent(N);
@@ -305,7 +436,7 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
         for (int l = 0; l < 32; ++l)
             for (int i : ent[g * 32 + l]) {
                 eu.push_back(l);
-                es.push_back(i % 32);
+                es.push_back(half ? (i >> 1) % 32 : i % 32);  // shared-memory bank of the input's word
                 ei.push_back(i);
             }
         const int D = ei.empty() ? 0 : colour_group(32, eu, es, colour);
@@ -314,15 +445,17 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
         for (size_t e = 0; e < ei.size(); ++e) order[g * 32 + eu[e]][colour[e]] = ei[e];
     }
     if (K > kBitsMaxK) return 0;
-    const int Kp = (K + 7) / 8 * 8;
-    // [group][step/8][lane] uint4 = 8 indices of 16 bits
-    std::vector<uint16_t> idx((size_t)ngroups * Kp * 32);
+    const int Kp = half ? (K + 15) / 16 * 16 : (K + 7) / 8 * 8;
+    // [group][step/8][lane] uint4 = 8 indices of 16 bits (row tiles) or
+    // [group][step/4][lane] uint4 = 4 indices of 32 bits (MMA tiles)
+    std::vector<uint16_t> idx(half ? 0 : (size_t)ngroups * Kp * 32);
+    std::vector<uint32_t> idx32(half ? (size_t)ngroups * Kp * 32 : 0);
     for (int g = 0; g < ngroups; ++g)
         for (int t = 0; t < Kp; ++t) {
             uint32_t used = 0;
             for (int l = 0; l < 32; ++l) {
                 const auto &o = order[g * 32 + l];
-                if (t < (int)o.size() && o[t] >= 0) used |= 1u << (o[t] % 32);
+                if (t < (int)o.size() && o[t] >= 0) used |= 1u << (half ? (o[t] >> 1) % 32 : o[t] % 32);
             }
             for (int l = 0; l < 32; ++l) {
                 const auto &o = order[g * 32 + l];
@@ -333,17 +466,20 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
                     int b = 0;  // a zero word in a bank no real entry of this step uses
                     while (used & (1u << b)) ++b;
                     used |= 1u << b;
-                    i = N + ((b - N % 32) + 32) % 32;
+                    i = half ? N + 2 * (((b - (N / 2) % 32) + 32) % 32) : N + ((b - N % 32) + 32) % 32;
                 }
-                idx[(((size_t)g * (Kp / 8) + t / 8) * 32 + l) * 8 + t % 8] = (uint16_t)i;
+                if (half) idx32[(((size_t)g * (Kp / 4) + t / 4) * 32 + l) * 4 + t % 4] = (uint32_t)i;
+                else idx[(((size_t)g * (Kp / 8) + t / 8) * 32 + l) * 8 + t % 8] = (uint16_t)i;
             }
         }
     void *d_idx = nullptr, *d_w = nullptr;
-    CSP_CUDA(cudaMalloc(&d_idx, idx.size() * sizeof(uint16_t)));
+    const size_t ibytes = half ? idx32.size() * sizeof(uint32_t) : idx.size() * sizeof(uint16_t);
+    CSP_CUDA(cudaMalloc(&d_idx, ibytes));
     owned.push_back(d_idx);
     CSP_CUDA(cudaMalloc(&d_w, (size_t)N * sizeof(float)));
     owned.push_back(d_w);
-    CSP_CUDA(cudaMemcpy(d_idx, idx.data(), idx.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    CSP_CUDA(cudaMemcpy(d_idx, half ? (const void *)idx32.data() : (const void *)idx.data(), ibytes,
+                        cudaMemcpyHostToDevice));
     CSP_CUDA(cudaMemcpy(d_w, w.data(), (size_t)N * sizeof(float), cudaMemcpyHostToDevice));
     nd.l0_idx = (const uint4 *)d_idx;
     nd.l0_w = (const float *)d_w;
@@ -351,14 +487,17 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
     return 0;
 }
 
-int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms, int max_n) {
+int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, bool mma, unsigned long long *launches, int sms,
+            int max_n) {
     using F = void (*)(const NetDev *, int, int, unsigned long long *);
     static const F fns[3] = {k_layer0_bits<float>, k_layer0_bits<__half>, k_layer0_bits<__nv_bfloat16>};
-    k.fn = (void *)fns[prec];
-    k.smem = (size_t)(max_n + 32) * 4;
+    static const F fns16[3] = {nullptr, k_layer0_bits16<__half>, k_layer0_bits16<__nv_bfloat16>};
+    CSP_CHECK(!mma || prec != COSPDNN_PREC_FP32, COSPDNN_ERR_UNSUPPORTED, "l0_spec: FP32 MMA-tile net");
+    k.fn = (void *)(mma ? fns16[prec] : fns[prec]);
+    k.smem = mma ? (size_t)(max_n + 64) * 2 : (size_t)(max_n + 32) * 4;
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
-    k.grid = dim3(2 * sms);
-    k.block = dim3(kBitsThreads);
+    k.grid = dim3(mma ? sms : 2 * sms);
+    k.block = dim3(mma ? kBits16Threads : kBitsThreads);
     k.arg(nets).arg(nnets).arg(prec).arg(launches);
     return COSPDNN_OK;
 }

@@ -7,14 +7,17 @@
 
 namespace cospdnn {
 
-// Builds the bit-count schedule of layer 0 of a row-tile net when every
-// output's weights are one value (zero entries ignored) and no output has
-// more than 63 of them; returns the steps per output (a multiple of 8), or 0
-// when the layer does not qualify (nothing is uploaded then).
+// Builds the bit-count schedule of layer 0 of a row-tile net (layout >= 4)
+// or an MMA-tile net (layout 1) when every output's weights are one value
+// (zero entries ignored) and no output has more than 63 of them; sets
+// nd.l0_k to the steps per output (a multiple of 8, or of 16 for MMA tiles),
+// left 0 when the layer does not qualify (nothing is uploaded then).
 int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
-             int N, int prec, int TR, NetDev &nd, std::vector<void *> &owned);
-// Launch of the bit-count kernel for the qualifying nets of precision `prec`.
-int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int sms, int max_n);
+             int N, int prec, int layout, NetDev &nd, std::vector<void *> &owned);
+// Launch of the bit-count kernel for the qualifying nets of precision `prec`
+// (mma: the MMA-tile nets, 16-bit precisions only).
+int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, bool mma, unsigned long long *launches, int sms,
+            int max_n);
 // Input rows (U8 or packed bits, row-major) as bit planes: word (unit, f)
 // holds feature f of rows 32*unit .. 32*unit+31 (bit r = row 32*unit+r is
 // non-zero; rows past `rows` are 0); also each row's max value (err0 = 0,

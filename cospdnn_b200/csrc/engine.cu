@@ -142,7 +142,9 @@ __global__ void k_convert_pieces(const uint8_t *__restrict__ src, int rows, int 
 // then every 16-feature block is written as one contiguous 4 KB operand.
 template <typename T, int FMT>
 __global__ void __launch_bounds__(256) k_convert_mma(const uint8_t *__restrict__ src, int rows, int N,
-                                                     T *__restrict__ y0) {
+                                                     T *__restrict__ y0, const int *__restrict__ skip_if_binary) {
+    // as k_convert_tile: a net counting layer 0 does not read this copy
+    if (skip_if_binary && *skip_if_binary == 0) return;
     __shared__ __align__(16) uint8_t slab[128][64];
     const int ng = (N + 63) / 64, nbk = N / 16;
     const int64_t units = (int64_t)((rows + 127) / 128) * ng;
@@ -451,16 +453,18 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
-    for (int prec = 0; prec < 3; ++prec) {
-        int max_n = 0;
-        for (const Net &n : e->nets)
-            if (n.dev.l0_k > 0 && n.d.precision == prec) max_n = std::max(max_n, n.d.neuron);
-        if (!max_n) continue;
-        KSpec k;
-        int rc = l0_spec(k, nets, nn, prec, launches, sms, max_n);
-        if (rc) return rc;
-        e->l0_specs.push_back(std::move(k));
-    }
+    for (int mma = 0; mma < 2; ++mma)
+        for (int prec = 0; prec < 3; ++prec) {
+            int max_n = 0;
+            for (const Net &n : e->nets)
+                if (n.dev.l0_k > 0 && n.d.precision == prec && (n.dev.layout == 1) == (mma == 1))
+                    max_n = std::max(max_n, n.d.neuron);
+            if (!max_n) continue;
+            KSpec k;
+            int rc = l0_spec(k, nets, nn, prec, mma == 1, launches, sms, max_n);
+            if (rc) return rc;
+            e->l0_specs.push_back(std::move(k));
+        }
     for (int prec : ks.tc) {
         KSpec k;
         int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, sms);
@@ -693,7 +697,10 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     for (Net &n : e->nets) {
         const int N = n.d.neuron, R = std::max(1, n.d.rows);
         n.ldev.resize(n.d.layers);
-        if (n.dev.kernel == COSPDNN_KERNEL_CUDA_CORE && n.dev.layout >= 4 && n.d.layers > 0) {
+        const bool l0_rows = n.dev.kernel == COSPDNN_KERNEL_CUDA_CORE && n.dev.layout >= 4;
+        const bool l0_mma = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 && n.dev.layout == 1 &&
+                            n.d.precision != COSPDNN_PREC_FP32;
+        if ((l0_rows || l0_mma) && n.d.layers > 0) {
             const HostLayer &h0 = n.layers[0];
             int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, n.dev.layout, n.dev, e->owned);
             if (rc) return rc;
@@ -843,6 +850,10 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     void *const y0dst = n.y0buf[back];
     const int blocks = std::min(65535, (R + 7) / 8);
     float *err0 = n.err0buf[back], *mx0 = n.mx0buf[back];
+    if (n.nbflag[back]) {
+        // binary unless the row maxima say otherwise (FP32 values: never counted)
+        CSP_CUDA(cudaMemsetAsync(n.nbflag[back], format == COSPDNN_INPUT_F32 ? 1 : 0, sizeof(int), s));
+    }
     if (n.dev.layout < 2 && format != COSPDNN_INPUT_F32) {
         // integer input into row-major or MMA-tile buffers
         const uint8_t *b = (const uint8_t *)src;
@@ -850,11 +861,15 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
         const int cb = (int)std::min<int64_t>((units + 255) / 256, 148 * 16);
         const int layout = n.dev.layout;
         const int mb = (int)std::min<int64_t>((int64_t)((R + 127) / 128) * ((N + 63) / 64), 148 * 8);
+        // a net counting layer 0 (MMA tiles): bit planes with the row maxima
+        // first, the compute-type copy only if the input is not binary
+        const int *skip = n.nbflag[back];
+        if (skip) l0_convert_bits(b, format, R, N, n.bitsbuf[back], err0, mx0, n.nbflag[back], s);
 #define CSP_PIECES(T)                                                                                        \
     do {                                                                                                     \
         if (layout == 1) {                                                                                   \
-            if (format == COSPDNN_INPUT_U8) k_convert_mma<T, COSPDNN_INPUT_U8><<<mb, 256, 0, s>>>(b, R, N, (T *)y0dst); \
-            else k_convert_mma<T, COSPDNN_INPUT_BITS><<<mb, 256, 0, s>>>(b, R, N, (T *)y0dst);                \
+            if (format == COSPDNN_INPUT_U8) k_convert_mma<T, COSPDNN_INPUT_U8><<<mb, 256, 0, s>>>(b, R, N, (T *)y0dst, skip); \
+            else if (!skip) k_convert_mma<T, COSPDNN_INPUT_BITS><<<mb, 256, 0, s>>>(b, R, N, (T *)y0dst, nullptr); \
         } else if (format == COSPDNN_INPUT_U8) {                                                             \
             k_convert_pieces<T, COSPDNN_INPUT_U8><<<cb, 256, 0, s>>>(b, R, N, layout, (T *)y0dst);        \
         } else {                                                                                             \
@@ -865,14 +880,12 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
         else if (n.d.precision == COSPDNN_PREC_FP16) CSP_PIECES(__half);
         else CSP_PIECES(__nv_bfloat16);
 #undef CSP_PIECES
-        if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
-        else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
+        if (!skip) {
+            if (format == COSPDNN_INPUT_U8) k_row_max<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
+            else k_row_max<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(b, R, N, err0, mx0, nullptr);
+        }
         CSP_CUDA(cudaGetLastError());
         return COSPDNN_OK;
-    }
-    if (n.nbflag[back]) {
-        // binary unless the row maxima say otherwise (FP32 values: never counted)
-        CSP_CUDA(cudaMemsetAsync(n.nbflag[back], format == COSPDNN_INPUT_F32 ? 1 : 0, sizeof(int), s));
     }
     if (n.dev.layout >= 2 && format != COSPDNN_INPUT_F32) {
         // integer input into row tiles

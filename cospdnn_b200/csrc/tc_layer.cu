@@ -154,7 +154,9 @@ struct Item {
 };
 
 __device__ __forceinline__ bool tc_net(const NetDev &nd, int prec) {
-    return nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.prec == prec && !nd.st->done;
+    // layer 0 of a net whose inputs were counted (bits_layer.cu) is done
+    return nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.prec == prec && !nd.st->done &&
+           !(nd.st->layer == 0 && nd.st->l0_bits);
 }
 // Work items of this layer (tile-major, so CTAs running at the same time share
 // the row tile's A operands in L2).
