@@ -320,13 +320,15 @@ def test_engine_next_input_set_during_run(cs):
         check_parity(r, ref, L)
 
 
-@pytest.mark.parametrize("n,prec,rows", [(1024, 1, 333), (4096, 1, 5), (16384, 2, 97), (1024, 0, 333),
-                                         (2048, 0, 64), (512, 1, 333)])
-def test_layer0_bit_count_matches_general_kernel(cs, n, prec, rows):
+@pytest.mark.parametrize("n,prec,rows,kernel", [(1024, 1, 333, 1), (4096, 1, 5, 1), (16384, 2, 97, 1),
+                                                (1024, 0, 333, 1), (2048, 0, 64, 1), (512, 1, 333, 1),
+                                                (4096, 1, 333, 2), (2048, 2, 17, 2), (1024, 1, 200, 2)])
+def test_layer0_bit_count_matches_general_kernel(cs, n, prec, rows, kernel):
     """Layer 0 by bit counting (binary inputs, one weight value per output)
     stores exactly what the general row-tile kernel stores: a one-layer net
     run on U8 and packed-bit inputs (counted) and on the same rows as FP32
-    (never counted); row tiles of 64, 32, 16, 8 and 4 rows.  Per-output
+    (never counted); row tiles of 64, 32, 16, 8 and 4 rows (CUDA-core nets,
+    32-row units) and MMA tiles (tcgen05 nets, 16-row units).  Per-output
     weight values differ (1/16 times 1, 2 or 3), so the kernel reads each
     output's own weight."""
     from oracle import pyoracle as po
@@ -337,7 +339,7 @@ def test_layer0_bit_count_matches_general_kernel(cs, n, prec, rows):
     b = np.float32(-0.3)
     ref = oracle_run([(cp, ri, vv)], y0, b)
     eng = cs.Engine(0)
-    nid = eng.add_net(n, 1, rows, float(b), 1e-5, prec, 1)
+    nid = eng.add_net(n, 1, rows, float(b), 1e-5, prec, kernel)
     eng.set_layer_csc(nid, 0, cp, ri, vv)
     eng.build()
     outs = []
