@@ -350,7 +350,8 @@ def main():
         traffic = DRAM_BYTES_PER_ROW[args.config] * rows_per_launch
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "layer kernel of the net (row-tile CUDA-core, tcgen05 or row-major gather)",
+                "kernel": "layer kernels of the net (bit-count layer 0 for binary inputs; row-tile CUDA-core, "
+                          "tcgen05 or row-major gather)",
                 "traffic_note": "DRAM bytes per launch scaled from an ncu capture of a smaller case "
                                 "(per input row) to this workload's average rows per layer launch",
                 "bytes_per_launch": tot_b / max(1, nit),
