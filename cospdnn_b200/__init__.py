@@ -223,6 +223,51 @@ class Engine:
 
 
 # ------------------------------------------------- reference host API mirror
+class NetworkC(C.Structure):
+    """cospdnn_network (include/cospdnn_b200.h)."""
+    _fields_ = [("desc", NetDesc), ("colptr", C.c_void_p), ("rowidx", C.c_void_p), ("vals", C.c_void_p),
+                ("y0", C.c_void_p), ("format", C.c_int), ("categories", C.c_void_p), ("count", C.c_void_p),
+                ("alive_per_layer", C.c_void_p)]
+
+
+def run_networks(networks, device=0):
+    """One call for any number of networks (cospdnn_run_networks).  Each item:
+    dict(neuron, layers (list of CSC (colptr, rowidx, vals)), y0 (uint8 or
+    float32 [rows][neuron]), bias, threshold=THRESHOLD, precision=PREC_FP16,
+    kernel=KERNEL_AUTO).  Returns ([dict(categories, alive)], device ms)."""
+    keep, structs, outs = [], [], []
+    for w in networks:
+        L = len(w["layers"])
+        y0 = np.ascontiguousarray(w["y0"])
+        fmt = INPUT_U8 if y0.dtype == np.uint8 else INPUT_F32
+        if fmt == INPUT_F32:
+            y0 = np.ascontiguousarray(y0, np.float32)
+        cps = [np.ascontiguousarray(cp, np.int32) for cp, _, _ in w["layers"]]
+        ris = [np.ascontiguousarray(ri, np.int32) for _, ri, _ in w["layers"]]
+        vvs = [np.ascontiguousarray(vv, np.float32) for _, _, vv in w["layers"]]
+        P32, PF = C.POINTER(C.c_int32), C.POINTER(C.c_float)
+        acp = (P32 * L)(*[a.ctypes.data_as(P32) for a in cps])
+        ari = (P32 * L)(*[a.ctypes.data_as(P32) for a in ris])
+        avv = (PF * L)(*[a.ctypes.data_as(PF) for a in vvs])
+        rows = y0.shape[0]
+        cats = np.zeros(max(1, rows), np.int32)
+        cnt = np.zeros(1, np.int64)
+        alive = np.zeros(max(1, L), np.int64)
+        d = NetDesc(int(w["neuron"]), L, rows, float(w["bias"]), float(w.get("threshold", THRESHOLD)),
+                    int(w.get("precision", PREC_FP16)), int(w.get("kernel", KERNEL_AUTO)))
+        structs.append(NetworkC(d, C.cast(acp, C.c_void_p), C.cast(ari, C.c_void_p), C.cast(avv, C.c_void_p),
+                                y0.ctypes.data, fmt, cats.ctypes.data, cnt.ctypes.data, alive.ctypes.data))
+        keep += [y0, cps, ris, vvs, acp, ari, avv]
+        outs.append((cats, cnt, alive, L))
+    arr = (NetworkC * len(structs))(*structs)
+    ms = C.c_float()
+    L_ = lib()
+    L_.cospdnn_run_networks.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float)]
+    _check(L_.cospdnn_run_networks(C.addressof(arr), len(structs), int(device), C.byref(ms)))
+    res = [{"categories": cats[:int(cnt[0])].copy(), "alive": alive[:L].copy()} for cats, cnt, alive, L in outs]
+    return res, ms.value
+
+
 def test_graph_challenge_tc(input, weight, row_idx, ptr, fuse_list, batch, neuron, bias,
                             blocksize_c=16, blocksize_r=16, gpu_id=0, gpu_num=1,
                             precision=PREC_FP16, threshold=THRESHOLD, verbose=True):

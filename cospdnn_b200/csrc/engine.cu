@@ -1087,6 +1087,36 @@ extern "C" int cospdnn_engine_result_async(cospdnn_engine *e, int net, void *hos
     return COSPDNN_OK;
 }
 
+extern "C" int cospdnn_run_networks(const cospdnn_network *nets, int n, int device, float *ms) {
+    CSP_CHECK(nets && n > 0, COSPDNN_ERR_INVALID, "run_networks: no networks");
+    for (int i = 0; i < n; ++i) {
+        const cospdnn_network &w = nets[i];
+        CSP_CHECK(w.count && w.y0, COSPDNN_ERR_INVALID, "run_networks: null input or count");
+        CSP_CHECK(w.desc.layers <= 0 || (w.colptr && w.rowidx && w.vals), COSPDNN_ERR_INVALID,
+                  "run_networks: null layer arrays");
+        CSP_CHECK(w.desc.rows <= 0 || w.categories, COSPDNN_ERR_INVALID, "run_networks: null categories");
+    }
+    cospdnn_engine *e = nullptr;
+    int rc = cospdnn_engine_create(&e, device);
+    if (rc) return rc;
+    std::unique_ptr<cospdnn_engine, void (*)(cospdnn_engine *)> guard(e, cospdnn_engine_destroy);
+    std::vector<int> ids(n);
+    for (int i = 0; i < n && !rc; ++i) {
+        rc = cospdnn_engine_add_net(e, &nets[i].desc, &ids[i]);
+        for (int l = 0; l < nets[i].desc.layers && !rc; ++l)
+            rc = cospdnn_engine_set_layer_csc(e, ids[i], l, nets[i].colptr[l], nets[i].rowidx[l], nets[i].vals[l]);
+    }
+    if (!rc) rc = cospdnn_engine_build(e);
+    for (int i = 0; i < n && !rc; ++i) rc = cospdnn_engine_set_input(e, ids[i], nets[i].y0, nets[i].format, 0, nullptr);
+    float t = 0.0f;
+    if (!rc) rc = cospdnn_engine_run_timed(e, nullptr, &t);
+    for (int i = 0; i < n && !rc; ++i)
+        rc = cospdnn_engine_result(e, ids[i], nets[i].categories, nets[i].count, nets[i].alive_per_layer, nullptr,
+                                   nullptr);
+    if (!rc && ms) *ms = t;
+    return rc;
+}
+
 extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, int max_iters,
                                              float *layer_ms, int *iters) {
     CSP_CHECK(e && layer_ms && iters && max_iters > 0, COSPDNN_ERR_INVALID, "profile_layers: bad argument");

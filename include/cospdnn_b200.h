@@ -172,6 +172,29 @@ int cospdnn_engine_build(cospdnn_engine *e);
  * the run before it has finished (the buffers alternate). */
 int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *y0, int format,
                              int on_device, void *stream);
+/* ------------------------------------------------------------------------
+ * One call for the persistent multi-network launch (the whole host loop of
+ * test_graph_challenge_tc / _co, src/cospdnn.cuh:14-35, for any number of
+ * networks): an engine on `device` is built from each network's CSC layers,
+ * the inputs are set, every network runs in one graph launch, and each
+ * network's results are copied back; the engine is destroyed before the
+ * call returns.  Networks given as BCSC + fuse rows go through
+ * cospdnn_engine_set_layer_bcsc instead.  *ms (may be NULL) receives the
+ * device time of the run, as cospdnn_engine_run_timed.
+ */
+typedef struct {
+    cospdnn_net_desc desc;          /* sizes, bias, threshold, precision, kernel */
+    const int32_t *const *colptr;   /* [layers] CSC column pointers, neuron + 1 each */
+    const int32_t *const *rowidx;   /* [layers] row (input) indices */
+    const float *const *vals;       /* [layers] weights */
+    const void *y0;                 /* host rows in `format` (COSPDNN_INPUT_*) */
+    int format;
+    int32_t *categories;            /* out: surviving original rows, room for desc.rows */
+    int64_t *count;                 /* out: number of categories */
+    int64_t *alive_per_layer;       /* out (may be NULL): rows kept after each layer */
+} cospdnn_network;
+int cospdnn_run_networks(const cospdnn_network *nets, int n, int device, float *ms);
+
 /* Number of CUDA devices visible to this process (0 when none, or on error);
  * replaces cudaGetDeviceCount in the reference's multi-GPU launcher
  * (src/cospdnn.cpp:155-163). */

@@ -377,3 +377,20 @@ def test_layer0_bit_count_falls_back(cs):
         eng.run()
         check_parity(eng.result(nid), ref, 2)
         eng.close()
+
+
+def test_run_networks_one_call(cs):
+    """cospdnn_run_networks: three networks of different widths, depths,
+    precisions and kernels (row tiles, MMA tiles) in one call, U8 and FP32
+    inputs, each equal to the FP64 oracle."""
+    from netgen import make_random_net
+    a_csc, a_y0, a_b = make_net(1024, 5, 300, seed=71, dlo=0.2, dhi=0.4)
+    b_csc, b_y0, b_b = make_random_net(512, 3, 120, seed=72)
+    c_csc, c_y0, c_b = make_net(4096, 4, 200, seed=73, dlo=0.2, dhi=0.4, kind="r1")
+    nets = [dict(neuron=1024, layers=a_csc, y0=a_y0, bias=a_b, precision=cs.PREC_FP16),
+            dict(neuron=512, layers=b_csc, y0=b_y0.astype(np.float32), bias=b_b, precision=cs.PREC_FP32),
+            dict(neuron=4096, layers=c_csc, y0=c_y0, bias=c_b, precision=cs.PREC_BF16, kernel=cs.KERNEL_TCGEN05)]
+    res, ms = cs.run_networks(nets)
+    assert ms > 0
+    for r, (csc, y0, b) in zip(res, ((a_csc, a_y0, a_b), (b_csc, b_y0, b_b), (c_csc, c_y0, c_b))):
+        check_parity(r, oracle_run(csc, y0, b), len(csc))
