@@ -182,6 +182,11 @@ __global__ void __launch_bounds__(256) k_convert_mma(const uint8_t *__restrict__
     }
 }
 
+// Stores a network descriptor passed by value (kernel arguments are copied at
+// launch, so the update is asynchronous: a copy from pageable host memory
+// would synchronize the stream first).
+__global__ void k_store_netdev(NetDev *dst, NetDev v) { *dst = v; }
+
 // Per-row max |input| (error 0) of integer inputs: one warp per row.
 // `nonbin` (may be NULL) is raised when a value is above 1.
 template <int FMT>
@@ -811,6 +816,9 @@ extern "C" int cospdnn_engine_set_input(cospdnn_engine *e, int net, const void *
     CSP_CHECK(e->built, COSPDNN_ERR_STATE, "set_input: build first");
     CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "set_input: bad net");
     CSP_CHECK(format >= 0 && format <= 2, COSPDNN_ERR_INVALID, "set_input: bad format");
+    // the conversion kernels read device rows with 8- and 16-byte loads
+    CSP_CHECK(!on_device || (uintptr_t)y0 % 16 == 0, COSPDNN_ERR_INVALID,
+              "set_input: device input must be 16-byte aligned");
     DeviceGuard g(e->device);
     Net &n = e->nets[net];
     const int N = n.d.neuron, R = n.d.rows;
@@ -953,8 +961,8 @@ int take_inputs(cospdnn_engine *e, cudaStream_t s) {
             n.dev.y0bits = n.bitsbuf[n.front];
             n.dev.y0nonbin = n.nbflag[n.front];
         }
-        // from pageable memory: the descriptor is staged before the call returns
-        CSP_CUDA(cudaMemcpyAsync(e->d_nets + i, &n.dev, sizeof(NetDev), cudaMemcpyHostToDevice, s));
+        k_store_netdev<<<1, 1, 0, s>>>(e->d_nets + i, n.dev);
+        CSP_CUDA(cudaGetLastError());
     }
     return COSPDNN_OK;
 }

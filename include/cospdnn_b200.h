@@ -162,8 +162,9 @@ int cospdnn_engine_build(cospdnn_engine *e);
 #define COSPDNN_INPUT_U8 0   /* [rows][neuron] bytes (binary images) */
 #define COSPDNN_INPUT_F32 1  /* [rows][neuron] float */
 #define COSPDNN_INPUT_BITS 2 /* [rows][neuron/8] bytes, bit j%8 of byte j/8, LSB first */
-/* Copies Y0 of one network (host pointer: pinned memory keeps it async) and
- * converts it to the compute type.  Asynchronous on `stream`.  Inputs are
+/* Copies Y0 of one network (host pointer: pinned memory keeps it async; a
+ * device pointer, on_device = 1, must be 16-byte aligned) and converts it to
+ * the compute type.  Asynchronous on `stream`.  Inputs are
  * double buffered: this fills the network's back buffers and the next run
  * (cospdnn_engine_run / _run_timed / _profile_layers) makes them current,
  * so the next batch can be set on another stream while a run is in flight.
