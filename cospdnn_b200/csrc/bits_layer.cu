@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
         if (blockIdx.x == 0 && threadIdx.x == 0) nd.st->l0_bits = 1;  // the row-tile kernel skips layer 0
         const int N = nd.N, R = nd.st->R, TR = nd.layout, K8 = nd.l0_k / 8;
         const int units = (R + 31) / 32, ngroups = N / 32;
+        const bool small = nd.l0_small != 0;
         const LayerDev &lw = nd.layers[0];
         T *out = (T *)nd.act[nd.st->in_buf ^ 1];
         const float bias = nd.bias;
@@ -151,8 +152,14 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                         const float cnt = __uint_as_float(__byte_perm(c4, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
                         const float z = fmaf(cnt, w, bias);
                         zmx[r] = fmaxf(zmx[r], z);
-                        zds[r] = fminf(zds[r], fabsf(z - 16.0f));
-                        ov[r] = act_traits<T>::from_f(clamp32(z));
+                        if (small) {
+                            // |z| <= 16: min |z - 16| is |max z - 16| (rounding of z - 16 is
+                            // monotone), taken from the row max below; no clamp at 32
+                            ov[r] = act_traits<T>::from_f(fmaxf(z, 0.0f));
+                        } else {
+                            zds[r] = fminf(zds[r], fabsf(z - 16.0f));
+                            ov[r] = act_traits<T>::from_f(clamp32(z));
+                        }
                     }
                 }
                 const int64_t row0 = (int64_t)u * 32;
@@ -173,10 +180,10 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
 #pragma unroll
             for (int r = 0; r < 32; ++r) {
                 const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
-                const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
-                if (lane == r) {
-                    atomicMax(&s_zmax[r], m);
-                    atomicMin(&s_zdist[r], d);
+                if (lane == r) atomicMax(&s_zmax[r], m);
+                if (!small) {
+                    const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
+                    if (lane == r) atomicMin(&s_zdist[r], d);
                 }
             }
             __syncthreads();
@@ -189,7 +196,7 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                     // bound plus the storage rounding when some output is within
                     // 16 + ez of 16
                     const float zm = ord2f(s_zmax[threadIdx.x]);
-                    const float zd = __uint_as_float(s_zdist[threadIdx.x]);
+                    const float zd = small ? fabsf(zm - 16.0f) : __uint_as_float(s_zdist[threadIdx.x]);
                     const float c = clamp32(zm);
                     const float ym = act_traits<T>::to_f(act_traits<T>::from_f(c));
                     float se = 0.0f;
@@ -394,8 +401,9 @@ __global__ void k_convert_bits(const uint8_t *__restrict__ src, int rows, int N,
 }  // namespace
 
 int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
-             int N, int prec, int layout, NetDev &nd, std::vector<void *> &owned) {
+             int N, int prec, int layout, float bias, NetDev &nd, std::vector<void *> &owned) {
     nd.l0_k = 0;
+    nd.l0_small = 0;
     nd.l0_idx = nullptr;
     nd.l0_w = nullptr;
     // row-tile nets: 32-bit words (32 rows), 16-bit indices, steps in 8s;
@@ -484,6 +492,9 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
     nd.l0_idx = (const uint4 *)d_idx;
     nd.l0_w = (const float *)d_w;
     nd.l0_k = Kp;
+    double zb = 0.0;  // bound on |z| of every output
+    for (int j = 0; j < N; ++j) zb = std::max(zb, std::fabs((double)w[j]) * (double)ent[j].size());
+    nd.l0_small = zb + std::fabs((double)bias) <= 16.0 ? 1 : 0;
     return 0;
 }
 

@@ -13,7 +13,7 @@ namespace cospdnn {
 // nd.l0_k to the steps per output (a multiple of 8, or of 16 for MMA tiles),
 // left 0 when the layer does not qualify (nothing is uploaded then).
 int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
-             int N, int prec, int layout, NetDev &nd, std::vector<void *> &owned);
+             int N, int prec, int layout, float bias, NetDev &nd, std::vector<void *> &owned);
 // Launch of the bit-count kernel for the qualifying nets of precision `prec`
 // (mma: the MMA-tile nets, 16-bit precisions only).
 int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, bool mma, unsigned long long *launches, int sms,

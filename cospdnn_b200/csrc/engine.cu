@@ -707,7 +707,8 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
                             n.d.precision != COSPDNN_PREC_FP32;
         if ((l0_rows || l0_mma) && n.d.layers > 0) {
             const HostLayer &h0 = n.layers[0];
-            int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, n.dev.layout, n.dev, e->owned);
+            int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, n.dev.layout, n.d.bias, n.dev,
+                              e->owned);
             if (rc) return rc;
             if (n.dev.l0_k > 0) {
                 for (int b = 0; b < 2; ++b) {

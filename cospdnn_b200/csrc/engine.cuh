@@ -111,6 +111,7 @@ struct NetDev {
     const uint4 *l0_idx;     // [N/32][l0_k/8][32] x 8 input indices (16 bits)
     const float *l0_w;       // [N] the output's weight in the compute type
     int l0_k;
+    int l0_small;            // every layer-0 output has |z| <= 16 (max_j |w_j| nnz_j + |bias|)
 };
 
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
