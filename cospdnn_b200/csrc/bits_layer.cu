@@ -432,8 +432,14 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
         if (prec == COSPDNN_PREC_FP16) w[j] = __half2float(__float2half_rn(w[j]));
         else if (prec == COSPDNN_PREC_BF16) w[j] = __bfloat162float(__float2bfloat16_rn(w[j]));
     }
-    // per warp of 32 outputs: edge colouring outputs x banks
+    // per warp of 32 outputs: edge colouring outputs x banks, so that the
+    // lanes of a step read distinct banks; when outputs share their inputs
+    // (dense blocks) the colouring needs many more steps than entries, and
+    // ascending input order is better: lanes reading the same word are served
+    // by one broadcast
     const int ngroups = N / 32;
+    int Knat = 1;
+    for (int j = 0; j < N; ++j) Knat = std::max(Knat, (int)ent[j].size());
     std::vector<std::vector<int>> order(N);
     int K = 1;
     std::vector<int> eu, es, colour;
@@ -452,7 +458,12 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
         for (int l = 0; l < 32; ++l) order[g * 32 + l].assign(D, -1);
         for (size_t e = 0; e < ei.size(); ++e) order[g * 32 + eu[e]][colour[e]] = ei[e];
     }
-    if (K > kBitsMaxK) return 0;
+    if (4 * K > 5 * Knat) {  // more than 25% padding: ascending order instead
+        K = Knat;
+        for (int j = 0; j < N; ++j) order[j] = ent[j];  // rows ascending within each column (CSC)
+    }
+    // padding words are zero, so only the real entries (<= 63 per output)
+    // reach the six counters; the number of steps is not limited
     const int Kp = half ? (K + 15) / 16 * 16 : (K + 7) / 8 * 8;
     // [group][step/8][lane] uint4 = 8 indices of 16 bits (row tiles) or
     // [group][step/4][lane] uint4 = 4 indices of 32 bits (MMA tiles)

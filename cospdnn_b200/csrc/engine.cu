@@ -365,6 +365,23 @@ double block_fill(const Net &net) {
     return blocks > 0.0 ? nnz / (blocks * 256.0) : 0.0;
 }
 
+// Distinct aligned 16x16 blocks per block column of one layer, on average.
+double blocks_per_column(const HostLayer &h, int N) {
+    const int nb = (N + 15) / 16;
+    std::vector<int> mark(nb, -1);
+    double blocks = 0.0;
+    for (int c = 0; c < nb; ++c)
+        for (int j = c * 16; j < std::min(N, c * 16 + 16); ++j)
+            for (int p = h.colptr[j]; p < h.colptr[j + 1]; ++p) {
+                const int b = h.rowidx[p] / 16;
+                if (mark[b] != c) {
+                    mark[b] = c;
+                    blocks += 1.0;
+                }
+            }
+    return blocks / nb;
+}
+
 // Kernel for COSPDNN_KERNEL_AUTO.  The CUDA-core row-tile kernel costs about
 // the same per nonzero whatever the sparsity pattern; a tcgen05 MMA costs a
 // fixed 16x16 block whatever its fill.  Measured on one B200 (4096 neurons,
@@ -703,8 +720,13 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         const int N = n.d.neuron, R = std::max(1, n.d.rows);
         n.ldev.resize(n.d.layers);
         const bool l0_rows = n.dev.kernel == COSPDNN_KERNEL_CUDA_CORE && n.dev.layout >= 4;
+        // tcgen05 nets: counting pays when layer 0's blocks are sparse (measured
+        // on one B200 at 4096 neurons, 60000 rows: counting 0.58 ms, the MMA
+        // kernel 0.26 + 0.064 ms per block per column; dense-block layers
+        // such as R1's, 2 blocks per column, stay on tcgen05)
         const bool l0_mma = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 && n.dev.layout == 1 &&
-                            n.d.precision != COSPDNN_PREC_FP32;
+                            n.d.precision != COSPDNN_PREC_FP32 && n.d.layers > 0 &&
+                            blocks_per_column(n.layers[0], N) >= 6.0;
         if ((l0_rows || l0_mma) && n.d.layers > 0) {
             const HostLayer &h0 = n.layers[0];
             int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, n.dev.layout, n.d.bias, n.dev,
