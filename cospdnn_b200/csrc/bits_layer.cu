@@ -433,10 +433,9 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
         else if (prec == COSPDNN_PREC_BF16) w[j] = __bfloat162float(__float2bfloat16_rn(w[j]));
     }
     // per warp of 32 outputs: edge colouring outputs x banks, so that the
-    // lanes of a step read distinct banks; when outputs share their inputs
-    // (dense blocks) the colouring needs many more steps than entries, and
-    // ascending input order is better: lanes reading the same word are served
-    // by one broadcast
+    // lanes of a step read distinct banks, or ascending input order when that
+    // costs fewer wavefronts (outputs sharing their inputs, as in dense
+    // blocks: lanes reading the same word are served by one broadcast)
     const int ngroups = N / 32;
     int Knat = 1;
     for (int j = 0; j < N; ++j) Knat = std::max(Knat, (int)ent[j].size());
@@ -458,7 +457,30 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
         for (int l = 0; l < 32; ++l) order[g * 32 + l].assign(D, -1);
         for (size_t e = 0; e < ei.size(); ++e) order[g * 32 + eu[e]][colour[e]] = ei[e];
     }
-    if (4 * K > 5 * Knat) {  // more than 25% padding: ascending order instead
+    // shared-memory wavefronts of both orders: the coloured one costs one per
+    // step; ascending order costs, per step, the largest number of distinct
+    // words one bank serves (lanes reading the same word share a broadcast)
+    double cost_col = (double)ngroups * K, cost_nat = 0.0;
+    {
+        std::vector<int> seen(32 * 32);
+        for (int g = 0; g < ngroups; ++g)
+            for (int t = 0; t < Knat; ++t) {
+                int nb[32] = {0}, worst = 1;
+                int ns = 0;
+                for (int l = 0; l < 32; ++l) {
+                    const auto &e = ent[g * 32 + l];
+                    if (t >= (int)e.size()) continue;
+                    const int word = half ? e[t] >> 1 : e[t], bank = word % 32;
+                    bool dup = false;
+                    for (int q = 0; q < ns; ++q) dup |= seen[q] == word;
+                    if (dup) continue;
+                    seen[ns++] = word;
+                    worst = std::max(worst, ++nb[bank]);
+                }
+                cost_nat += worst;
+            }
+    }
+    if (cost_nat < cost_col) {
         K = Knat;
         for (int j = 0; j < N; ++j) order[j] = ent[j];  // rows ascending within each column (CSC)
     }
