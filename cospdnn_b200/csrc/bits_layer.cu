@@ -2,26 +2,32 @@
 // images and every output's weights are one value (1/16 in the Graph
 // Challenge networks), so an output of layer 0 is
 //     z = bias + w_j * (number of its inputs that are 1),
-// an exact integer count.  The kernel counts 32 rows at once: the inputs are
-// stored as bit planes (one 32-bit word per feature and 32 rows, built with
-// the rest of the input conversion), a CTA stages one unit of 32 rows (4
-// bytes per feature) in shared memory, and lane j of a warp adds the words
-// of output j's inputs into six bit-sliced counters (carry-save adders,
-// Harley-Seal: about 2.4 logic instructions per word for 32 rows).  The
-// counts are moved into bytes four rows at a time (a multiply spreads 4 bits
-// of a plane into 4 bytes), then bias, clamp and the store in the compute
-// type follow the epilogue of the kernel the net uses otherwise, with its
-// per-row statistics for the keep/prune decision, so the stored values and
-// the rows sent to the FP64 recheck are the same as without counting.  Shared-memory traffic per output
-// and 32 rows is 32 words against 32 * 32 rows of 16-bit values in the
-// general kernel.
-//
-// Entry schedule: the 32 outputs of a warp read their inputs' words at
-// step t from 32 distinct banks (edge colouring of outputs x banks, as in the
-// row-tile kernel), padded with zero words placed in the free banks.
-// Binary inputs are checked per input (U8 maxima, the packed-bit format is
-// binary); otherwise, and for FP32 input values, layer 0 runs on the general
-// kernel.
+// an exact integer count.  The inputs are stored as bit planes (one 32-bit
+// word per feature and 32 rows, made by the input conversion, which then
+// skips the compute-type copy).  A CTA stages one unit of rows in shared
+// memory and lane j of a warp adds the words of output j's inputs into six
+// bit-sliced counters (carry-save adders, Harley-Seal: about 2.4 logic
+// instructions per word); the counts are moved into bytes four rows at a
+// time (a multiply spreads 4 bits of a plane into 4 bytes) and turned into
+// floats exactly by a byte permute.  Bias, clamp and the store in the
+// compute type follow the epilogue of the kernel the net uses otherwise, with
+// its per-row statistics for the keep/prune decision, so the stored values
+// and the rows sent to the FP64 recheck are the same as without counting.
+//   k_layer0_bits    row-tile nets: units of 32 rows (4 bytes per feature);
+//                    shared-memory traffic per output and 32 rows is 32
+//                    words against 32 x 32 16-bit values in the row-tile
+//                    kernel.
+//   k_layer0_bits16  MMA-tile (tcgen05) nets: units of 16 rows (2 bytes per
+//                    feature, so 65536 features fit in shared memory), two
+//                    entries' words packed per 32-bit word, values stored into
+//                    the MMA operand tiles.
+// Entry schedule: per warp of 32 outputs, either an edge colouring of
+// outputs x banks (the lanes of a step read 32 distinct banks; padding reads
+// zero words placed in free banks) or ascending input order, whichever costs
+// fewer shared-memory wavefronts (ascending order is conflict-free for XOR
+// masks and broadcast-friendly for dense blocks).  Binary inputs are checked
+// per input (U8 maxima; the packed-bit format is binary); other inputs, FP32
+// values, and layers whose outputs mix weight values take the general kernels.
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
@@ -35,7 +41,7 @@ namespace {
 
 constexpr int kBitsThreads = 256;
 constexpr int kBitsWarps = kBitsThreads / 32;
-constexpr int kBitsMaxK = 63;  // six bit-sliced counters
+constexpr int kBitsMaxK = 63;  // real entries per output: six bit-sliced counters
 
 __device__ __forceinline__ void csa(uint32_t &h, uint32_t &l, uint32_t a, uint32_t b, uint32_t c) {
     const uint32_t u = a ^ b;
