@@ -19,6 +19,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -101,7 +102,10 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # raw samples: $COSPDNN_CLOCKS_DIR if set, else the temporary directory
+        # (the JSON line carries their summary)
+        out = os.environ.get("COSPDNN_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"cospdnn_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
