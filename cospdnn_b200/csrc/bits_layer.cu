@@ -7,9 +7,9 @@
 // skips the compute-type copy).  A CTA stages one unit of rows in shared
 // memory and lane j of a warp adds the words of output j's inputs into six
 // bit-sliced counters (carry-save adders, Harley-Seal: about 2.4 logic
-// instructions per word); the counts are moved into bytes four rows at a
-// time (a multiply spreads 4 bits of a plane into 4 bytes) and turned into
-// floats exactly by a byte permute.  Bias, clamp and the store in the
+// instructions per word); the counters are turned into one byte per row by
+// an 8x8 bit transpose across the planes (three rounds of delta swaps) and
+// into floats exactly by a byte permute.  Bias, clamp and the store in the
 // compute type follow the epilogue of the kernel the net uses otherwise, with
 // its per-row statistics for the keep/prune decision, so the stored values
 // and the rows sent to the FP64 recheck are the same as without counting.
@@ -66,15 +66,46 @@ __device__ __forceinline__ void add8(uint32_t (&p)[6], const uint32_t (&x)[8]) {
     p[5] ^= c16;  // counts stay below 64
 }
 
-// Counts of rows 4q..4q+3, one per byte.
-__device__ __forceinline__ uint32_t counts4(const uint32_t (&p)[6], int q) {
-    uint32_t c = 0;
+// The counters as bytes: byte g of c[k] = the count at bit position 8g + k.
+// Planes 0..5 (with 6 and 7 zero) hold, at each bit position, one bit of an
+// 8-bit count; transposing the 8x8 bit matrix of each byte column across the
+// eight words (three rounds of delta swaps of 4-, 2- and 1-bit blocks) gives
+// each position's count as a byte.
+__device__ __forceinline__ void counts8(const uint32_t (&p)[6], uint32_t (&c)[8]) {
 #pragma unroll
-    for (int b = 0; b < 6; ++b) {
-        const uint32_t nib = (p[b] >> (4 * q)) & 0xFu;
-        c |= (nib * (0x00204081u << b)) & (0x01010101u << b);  // bit i of nib -> bit b of byte i
+    for (int b = 0; b < 6; ++b) c[b] = p[b];
+    c[6] = c[7] = 0u;
+#pragma unroll
+    for (int d = 4; d >= 1; d >>= 1) {
+        const uint32_t m = d == 4 ? 0x0F0F0F0Fu : d == 2 ? 0x33333333u : 0x55555555u;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (i & d) continue;
+            const uint32_t t = ((c[i] >> d) ^ c[i + d]) & m;
+            c[i + d] ^= t;
+            c[i] ^= t << d;
+        }
     }
-    return c;
+}
+
+// byte g of a counts word as the float 2^23 + count (the byte as its mantissa)
+__device__ __forceinline__ uint32_t count_bits(uint32_t c, int g) { return __byte_perm(c, 0x4B000000u, 0x7440u | g); }
+
+// z = count * w + bias for two counts given as 2^23 + count: the count is
+// recovered exactly by subtracting 2^23, in two sm_100 packed instructions
+// (add.rn.f32x2, fma.rn.f32x2: each half one IEEE operation, identical to
+// the scalar subtraction and fmaf)
+__device__ __forceinline__ void z_pair(uint32_t c0, uint32_t c1, float w, float bias, float &z0, float &z1) {
+    asm("{\n\t.reg .b64 x, m, w, b;\n\t"
+        "mov.b64 x, {%2, %3};\n\t"
+        "mov.b64 m, {%6, %6};\n\t"
+        "add.rn.f32x2 x, x, m;\n\t"
+        "mov.b64 w, {%4, %4};\n\t"
+        "mov.b64 b, {%5, %5};\n\t"
+        "fma.rn.f32x2 x, x, w, b;\n\t"
+        "mov.b64 {%0, %1}, x;\n\t}"
+        : "=f"(z0), "=f"(z1)
+        : "r"(c0), "r"(c1), "f"(w), "f"(bias), "f"(-8388608.0f));
 }
 
 template <typename T>
@@ -97,6 +128,84 @@ __device__ __forceinline__ bool l0_net(const NetDev &nd, int prec) {
            !nd.st->done && nd.st->layer == 0 && nd.y0bits != nullptr && *nd.y0nonbin == 0;
 }
 
+// One unit of 32 rows for the warp's groups of 32 outputs: counts, outputs
+// stored, and the warp's row max z (and, unless SMALL, min |z - 16|) merged
+// into the CTA's row statistics.  SMALL: |z| <= 16, so min |z - 16| is
+// |max z - 16| (rounding of z - 16 is monotone), taken from the row max, and
+// there is no clamp at 32.
+template <typename T, bool SMALL>
+__device__ __forceinline__ void count_unit(const NetDev &nd, const uint32_t *s_bits, uint32_t *s_zmax,
+                                           uint32_t *s_zdist, int u, int N, int TR, int K8, int ngroups, T *out,
+                                           float bias) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float zmx[32], zds[SMALL ? 1 : 32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        zmx[r] = -INFINITY;
+        if constexpr (!SMALL) zds[r] = INFINITY;
+    }
+    for (int g = warp; g < ngroups; g += kBitsWarps) {
+        const int j = g * 32 + lane;
+        uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+        const uint4 *ent = nd.l0_idx + (int64_t)g * K8 * 32 + lane;
+        for (int t = 0; t < K8; ++t) {
+            const uint4 q = __ldg(ent + (int64_t)t * 32);
+            const uint32_t x[8] = {s_bits[q.x & 0xFFFFu], s_bits[q.x >> 16], s_bits[q.y & 0xFFFFu],
+                                   s_bits[q.y >> 16],     s_bits[q.z & 0xFFFFu], s_bits[q.z >> 16],
+                                   s_bits[q.w & 0xFFFFu], s_bits[q.w >> 16]};
+            add8(p, x);
+        }
+        const float w = nd.l0_w[j];
+        // rows 8b .. 8b+7 (byte b of counts words 0..7), each group of 8 stored at once
+        constexpr int V = Pack<T>::kPer16;  // values per 16-byte piece
+        uint32_t c[8];
+        counts8(p, c);
+        const int64_t row0 = (int64_t)u * 32;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            __align__(16) T ov[8];
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) {
+                float z[2];
+                z_pair(count_bits(c[k], b), count_bits(c[k + 1], b), w, bias, z[0], z[1]);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int r = 8 * b + k + h;
+                    zmx[r] = fmaxf(zmx[r], z[h]);
+                    if constexpr (SMALL) {
+                        ov[k + h] = act_traits<T>::from_f(fmaxf(z[h], 0.0f));
+                    } else {
+                        zds[r] = fminf(zds[r], fabsf(z[h] - 16.0f));
+                        ov[k + h] = act_traits<T>::from_f(clamp32(z[h]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k += V) {
+                if (TR >= V) {  // a 16-byte piece lies inside one tile
+                    *reinterpret_cast<uint4 *>(out + act_index(TR, N, row0 + 8 * b + k, j)) =
+                        *reinterpret_cast<const uint4 *>(ov + k);
+                } else {  // 16-bit values, tiles of 4 rows: two 8-byte pieces
+                    *reinterpret_cast<uint2 *>(out + act_index(TR, N, row0 + 8 * b + k, j)) =
+                        *reinterpret_cast<const uint2 *>(ov + k);
+                    *reinterpret_cast<uint2 *>(out + act_index(TR, N, row0 + 8 * b + k + 4, j)) =
+                        *reinterpret_cast<const uint2 *>(ov + k + 4);
+                }
+            }
+        }
+    }
+    // row max z and min |z - 16| over the warp's outputs, then over the CTA
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
+        if (lane == r) atomicMax(&s_zmax[r], m);
+        if constexpr (!SMALL) {
+            const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
+            if (lane == r) atomicMin(&s_zdist[r], d);
+        }
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kBitsThreads, 2)
     k_layer0_bits(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
@@ -104,7 +213,6 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
     extern __shared__ uint4 l0_smem[];
     uint32_t *s_bits = reinterpret_cast<uint32_t *>(l0_smem);
     __shared__ uint32_t s_zmax[32], s_zdist[32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
         if (!l0_net(nd, prec)) continue;
@@ -127,71 +235,10 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
                 }
             }
             __syncthreads();
-            float zmx[32], zds[32];
-#pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                zmx[r] = -INFINITY;
-                zds[r] = INFINITY;
-            }
-            for (int g = warp; g < ngroups; g += kBitsWarps) {
-                const int j = g * 32 + lane;
-                uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
-                const uint4 *ent = nd.l0_idx + (int64_t)g * K8 * 32 + lane;
-                for (int t = 0; t < K8; ++t) {
-                    const uint4 q = __ldg(ent + (int64_t)t * 32);
-                    const uint32_t x[8] = {s_bits[q.x & 0xFFFFu], s_bits[q.x >> 16], s_bits[q.y & 0xFFFFu],
-                                           s_bits[q.y >> 16],     s_bits[q.z & 0xFFFFu], s_bits[q.z >> 16],
-                                           s_bits[q.w & 0xFFFFu], s_bits[q.w >> 16]};
-                    add8(p, x);
-                }
-                const float w = nd.l0_w[j];
-                // the 32 rows' values (row r = 4q + k), then the stores
-                constexpr int V = Pack<T>::kPer16;  // values per 16-byte piece
-                __align__(16) T ov[32];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const uint32_t c4 = counts4(p, q);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int r = 4 * q + k;
-                        // byte k of c4 as the mantissa of 2^23 + count: exact, no conversion
-                        const float cnt = __uint_as_float(__byte_perm(c4, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
-                        const float z = fmaf(cnt, w, bias);
-                        zmx[r] = fmaxf(zmx[r], z);
-                        if (small) {
-                            // |z| <= 16: min |z - 16| is |max z - 16| (rounding of z - 16 is
-                            // monotone), taken from the row max below; no clamp at 32
-                            ov[r] = act_traits<T>::from_f(fmaxf(z, 0.0f));
-                        } else {
-                            zds[r] = fminf(zds[r], fabsf(z - 16.0f));
-                            ov[r] = act_traits<T>::from_f(clamp32(z));
-                        }
-                    }
-                }
-                const int64_t row0 = (int64_t)u * 32;
-#pragma unroll
-                for (int k = 0; k < 32 / V; ++k) {
-                    if (TR >= V) {  // a 16-byte piece lies inside one tile
-                        *reinterpret_cast<uint4 *>(out + act_index(TR, N, row0 + k * V, j)) =
-                            *reinterpret_cast<const uint4 *>(ov + k * V);
-                    } else {  // 16-bit values, tiles of 4 rows: two 8-byte pieces
-                        *reinterpret_cast<uint2 *>(out + act_index(TR, N, row0 + k * V, j)) =
-                            *reinterpret_cast<const uint2 *>(ov + k * V);
-                        *reinterpret_cast<uint2 *>(out + act_index(TR, N, row0 + k * V + 4, j)) =
-                            *reinterpret_cast<const uint2 *>(ov + k * V + 4);
-                    }
-                }
-            }
-            // row max z and min |z - 16| over the warp's outputs, then over the CTA
-#pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
-                if (lane == r) atomicMax(&s_zmax[r], m);
-                if (!small) {
-                    const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zds[r]));  // >= 0
-                    if (lane == r) atomicMin(&s_zdist[r], d);
-                }
-            }
+            if (small)
+                count_unit<T, true>(nd, s_bits, s_zmax, s_zdist, u, N, TR, K8, ngroups, out, bias);
+            else
+                count_unit<T, false>(nd, s_bits, s_zmax, s_zdist, u, N, TR, K8, ngroups, out, bias);
             __syncthreads();
             if (threadIdx.x < 32) {
                 const int p = u * 32 + threadIdx.x;
@@ -295,14 +342,17 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                     add8(p, x);
                 }
                 const float w = nd.l0_w[j];
+                uint32_t c[8];
+                counts8(p, c);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t c4 = counts4(p, q) + counts4(p, q + 4);  // even + odd entries (each <= 32)
+                for (int k = 0; k < 8; ++k) {
+                    const uint32_t s2 = c[k] + (c[k] >> 16);  // even + odd entries' counts (each <= 32)
+                    float zz[2];
+                    z_pair(count_bits(s2, 0), count_bits(s2, 1), w, bias, zz[0], zz[1]);
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int r = 4 * q + k;
-                        const float cnt = __uint_as_float(__byte_perm(c4, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
-                        const float z = fmaf(cnt, w, bias);
+                    for (int g = 0; g < 2; ++g) {
+                        const int r = 8 * g + k;
+                        const float z = zz[g];
                         const float cz = clamp32(z);
                         const T o = act_traits<T>::from_f(cz);
                         zmx[r] = fmaxf(zmx[r], z);

@@ -320,21 +320,23 @@ def test_engine_next_input_set_during_run(cs):
         check_parity(r, ref, L)
 
 
-@pytest.mark.parametrize("n,prec,rows,kernel", [(1024, 1, 333, 1), (4096, 1, 5, 1), (16384, 2, 97, 1),
-                                                (1024, 0, 333, 1), (2048, 0, 64, 1), (512, 1, 333, 1),
-                                                (4096, 1, 333, 2), (2048, 2, 17, 2), (1024, 1, 200, 2)])
-def test_layer0_bit_count_matches_general_kernel(cs, n, prec, rows, kernel):
+@pytest.mark.parametrize("n,prec,rows,kernel,scale", [
+    (1024, 1, 333, 1, 1), (4096, 1, 5, 1, 1), (16384, 2, 97, 1, 1), (1024, 0, 333, 1, 1), (2048, 0, 64, 1, 1),
+    (512, 1, 333, 1, 1), (4096, 1, 333, 2, 1), (2048, 2, 17, 2, 1), (1024, 1, 200, 2, 1),
+    (1024, 1, 333, 1, 16), (2048, 0, 64, 1, 16), (4096, 2, 97, 1, 16), (1024, 1, 200, 2, 16)])
+def test_layer0_bit_count_matches_general_kernel(cs, n, prec, rows, kernel, scale):
     """Layer 0 by bit counting (binary inputs, one weight value per output)
     stores exactly what the general row-tile kernel stores: a one-layer net
     run on U8 and packed-bit inputs (counted) and on the same rows as FP32
     (never counted); row tiles of 64, 32, 16, 8 and 4 rows (CUDA-core nets,
     32-row units) and MMA tiles (tcgen05 nets, 16-row units).  Per-output
     weight values differ (1/16 times 1, 2 or 3), so the kernel reads each
-    output's own weight."""
+    output's own weight; scale 16 makes them 1, 2 or 3, so that outputs pass
+    16 and the clamp at 32 (the kernel's path for |z| > 16)."""
     from oracle import pyoracle as po
     cp, ri, vv = po.masks_to_csc(po.xor_masks(59, 0, 0, n), n)
     col = np.repeat(np.arange(n), np.diff(cp))
-    vv = (vv * (1 + col % 3)).astype(np.float32)
+    vv = (vv * (1 + col % 3) * scale).astype(np.float32)
     y0 = po.input_binary(59, 0, rows, n, 0.1, 0.3)
     b = np.float32(-0.3)
     ref = oracle_run([(cp, ri, vv)], y0, b)
