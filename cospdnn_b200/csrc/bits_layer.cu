@@ -32,6 +32,7 @@
 #include <cmath>
 #include <type_traits>
 
+#include "bit_count.cuh"
 #include "bits_layer.cuh"
 #include "cc_layer.cuh"
 
@@ -42,51 +43,6 @@ namespace {
 constexpr int kBitsThreads = 256;
 constexpr int kBitsWarps = kBitsThreads / 32;
 constexpr int kBitsMaxK = 63;  // real entries per output: six bit-sliced counters
-
-__device__ __forceinline__ void csa(uint32_t &h, uint32_t &l, uint32_t a, uint32_t b, uint32_t c) {
-    const uint32_t u = a ^ b;
-    h = (a & b) | (u & c);
-    l = u ^ c;
-}
-
-// count += number of set bits among x[0..7] at every bit position
-__device__ __forceinline__ void add8(uint32_t (&p)[6], const uint32_t (&x)[8]) {
-    uint32_t twosA, twosB, foursA, foursB, eightsA;
-    csa(twosA, p[0], p[0], x[0], x[1]);
-    csa(twosB, p[0], p[0], x[2], x[3]);
-    csa(foursA, p[1], p[1], twosA, twosB);
-    csa(twosA, p[0], p[0], x[4], x[5]);
-    csa(twosB, p[0], p[0], x[6], x[7]);
-    csa(foursB, p[1], p[1], twosA, twosB);
-    csa(eightsA, p[2], p[2], foursA, foursB);
-    const uint32_t c8 = p[3] & eightsA;
-    p[3] ^= eightsA;
-    const uint32_t c16 = p[4] & c8;
-    p[4] ^= c8;
-    p[5] ^= c16;  // counts stay below 64
-}
-
-// The counters as bytes: byte g of c[k] = the count at bit position 8g + k.
-// Planes 0..5 (with 6 and 7 zero) hold, at each bit position, one bit of an
-// 8-bit count; transposing the 8x8 bit matrix of each byte column across the
-// eight words (three rounds of delta swaps of 4-, 2- and 1-bit blocks) gives
-// each position's count as a byte.
-__device__ __forceinline__ void counts8(const uint32_t (&p)[6], uint32_t (&c)[8]) {
-#pragma unroll
-    for (int b = 0; b < 6; ++b) c[b] = p[b];
-    c[6] = c[7] = 0u;
-#pragma unroll
-    for (int d = 4; d >= 1; d >>= 1) {
-        const uint32_t m = d == 4 ? 0x0F0F0F0Fu : d == 2 ? 0x33333333u : 0x55555555u;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (i & d) continue;
-            const uint32_t t = ((c[i] >> d) ^ c[i + d]) & m;
-            c[i + d] ^= t;
-            c[i] ^= t << d;
-        }
-    }
-}
 
 // byte g of a counts word as the float 2^23 + count (the byte as its mantissa)
 __device__ __forceinline__ uint32_t count_bits(uint32_t c, int g) { return __byte_perm(c, 0x4B000000u, 0x7440u | g); }
