@@ -75,6 +75,19 @@ def lib():
         L.cospdnn_engine_result.argtypes = [vp, C.c_int, i32p, i64p, i64p, i64p, vp]
         L.cospdnn_engine_final_values.argtypes = [vp, C.c_int, f32p, C.c_int64, vp]
         L.cospdnn_engine_launch_count.argtypes = [vp, i64p, vp]
+        # declared for every entry point: an undeclared size_t or pointer would
+        # be passed as a C int
+        L.cospdnn_version.argtypes = []
+        L.cospdnn_device_count.argtypes = []
+        L.cospdnn_device_count.restype = C.c_int
+        L.cospdnn_prune_compact_noalloc.argtypes = [vp, C.c_int, C.c_int, C.c_float, vp, vp, vp, vp, vp,
+                                                    C.c_uint, vp]
+        L.cospdnn_engine_run_timed.argtypes = [vp, vp, f32p]
+        L.cospdnn_engine_result_async.argtypes = [vp, C.c_int, vp, C.c_size_t, vp]
+        L.cospdnn_engine_profile_layers.argtypes = [vp, vp, C.c_int, f32p, ip]
+        L.cospdnn_run_networks.argtypes = [vp, C.c_int, C.c_int, f32p]
+        L.cospdnn_synth_input.argtypes = [vp, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.c_int64, C.c_double,
+                                          C.c_double, C.c_int, vp]
         _lib = L
     return _lib
 
@@ -261,9 +274,7 @@ def run_networks(networks, device=0):
         outs.append((cats, cnt, alive, L))
     arr = (NetworkC * len(structs))(*structs)
     ms = C.c_float()
-    L_ = lib()
-    L_.cospdnn_run_networks.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_float)]
-    _check(L_.cospdnn_run_networks(C.addressof(arr), len(structs), int(device), C.byref(ms)))
+    _check(lib().cospdnn_run_networks(C.addressof(arr), len(structs), int(device), C.byref(ms)))
     res = [{"categories": cats[:int(cnt[0])].copy(), "alive": alive[:L].copy()} for cats, cnt, alive, L in outs]
     return res, ms.value
 

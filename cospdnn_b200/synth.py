@@ -100,10 +100,7 @@ def input_rows(rows, neuron, seed, net=0, dlo=0.08, dhi=0.25, row0=0, fmt=0, dev
     from . import _check, _stream, lib
     cols = neuron if fmt == 0 else neuron // 8
     out = torch.empty((rows, cols), dtype=torch.uint8, device=f"cuda:{device}")
-    f = lib().cospdnn_synth_input
-    f.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.c_int64, C.c_double,
-                  C.c_double, C.c_int, C.c_void_p]
-    _check(f(out.data_ptr(), rows, neuron, seed, net, row0, dlo, dhi, fmt, _stream(stream)))
+    _check(lib().cospdnn_synth_input(out.data_ptr(), rows, neuron, seed, net, row0, dlo, dhi, fmt, _stream(stream)))
     return out
 
 

@@ -52,7 +52,6 @@ def test_run_networks_rejects_bad_arguments_without_gpu():
     import ctypes as C
     import cospdnn_b200 as cs
     L = cs.lib()
-    L.cospdnn_run_networks.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     assert L.cospdnn_run_networks(None, 1, 0, None) == cs.ERR_INVALID
     net = cs.NetworkC()  # all pointers NULL
     net.desc.neuron, net.desc.layers, net.desc.rows = 64, 1, 10

@@ -57,8 +57,6 @@ def test_noalloc_prune_matches_allocating_entry_twice():
         pytest.skip("no CUDA device")
     import cospdnn_b200 as cs
     fn = cs.lib().cospdnn_prune_compact_noalloc
-    fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                   C.c_void_p, C.c_uint, C.c_void_p]
     for call, (seed, n, batch, hilo) in enumerate([(1, 64, 3000, False), (2, 48, 1700, True)]):
         c, map_in = _case(seed, n, batch)
         (k0, cat0, mo0, a0), (k1, cat1, mo1, a1) = _run(cs, fn, c, map_in, hilo)
@@ -77,8 +75,6 @@ def test_noalloc_prune_rejects_oversized_batch():
         pytest.skip("no CUDA device")
     import cospdnn_b200 as cs
     fn = cs.lib().cospdnn_prune_compact_noalloc
-    fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                   C.c_void_p, C.c_uint, C.c_void_p]
     dummy = torch.zeros(16, dtype=torch.int32, device="cuda")
     p = C.c_void_p(dummy.data_ptr())
     rc = fn(p, 4, (1 << 20) + 1, C.c_float(1e-5), p, p, None, p, p, 0, None)
