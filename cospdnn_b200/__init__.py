@@ -55,6 +55,7 @@ def lib():
         vp, ip, i32p, i64p, f32p = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int32), \
             C.POINTER(C.c_int64), C.POINTER(C.c_float)
         L.cospdnn_last_error.restype = C.c_char_p
+        L.cospdnn_last_error.argtypes = []
         L.cospdnn_version.restype = C.c_int
         L.cospdnn_layer.argtypes = [vp, vp, vp, vp, vp, vp, C.c_float, C.c_int, C.c_int, C.c_int,
                                     C.c_int, C.c_int, C.c_uint, vp]

@@ -1,5 +1,6 @@
-"""The C-ABI library loads and exports every function include/*.h declares
-(no compute calls: this runs without a GPU)."""
+"""The C-ABI library loads and exports every function include/*.h declares,
+each with its argument types declared in the ctypes layer (no compute calls:
+this runs without a GPU)."""
 import glob
 import os
 import re
@@ -30,6 +31,9 @@ def test_library_exports(name):
     import cospdnn_b200
     L = cospdnn_b200.lib()
     assert hasattr(L, name), f"{name} declared in include/ but not exported"
+    # the Python layer declares the argument types of every entry point, so
+    # no size_t or pointer argument goes through as a C int
+    assert getattr(L, name).argtypes is not None, name
 
 
 def test_version_and_error_string():
