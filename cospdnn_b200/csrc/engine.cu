@@ -1158,7 +1158,13 @@ extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, in
     if (rc) return rc;
     cudaEvent_t a, b;
     CSP_CUDA(cudaEventCreate(&a));
-    CSP_CUDA(cudaEventCreate(&b));
+    {
+        const cudaError_t err = cudaEventCreate(&b);
+        if (err != cudaSuccess) {
+            cudaEventDestroy(a);
+            return cuda_fail(err, "profile_layers: event");
+        }
+    }
     rc = launch(e->k0, s);
     int it = 0;
     std::vector<NetState> st(e->nets.size());
