@@ -21,11 +21,12 @@ W'[u'][v] = W[order[u']][v] with fuse[l][u'] = order[u'], the same product.
 A layer keeps the identity order when the reordering does not reduce its
 greedy block count.
 
-    python -m cospdnn_b200.reorder SRC DST neuron layers
+    python -m cospdnn_b200.reorder SRC DST neuron layers [--workers N]
 
 reads SRC/sparse-images-N.tsv and SRC/neuronN/N-l{l}.tsv (raw weights, rows =
 inputs, 1-based) and writes DST with the reordered weights, the same images
-and DST/fuse_matrix/neuronN/N_L_fuse.tsv.
+and DST/fuse_matrix/neuronN/N_L_fuse.tsv; layers are reordered in N processes
+(default: one per layer, up to the host's cores).
 """
 import os
 import shutil
@@ -47,22 +48,45 @@ def greedy_blocks(rows, cols, neuron, block=BLOCK):
     non-zeros at (rows, cols) (src/utils/matrix.h:1200-1269): non-zeros in
     column-major order; a block column starts at the first column past the
     previous one and spans `block` columns; a non-zero whose row no block of
-    its block column covers opens a block at that row, spanning `block` rows."""
+    its block column covers opens a block at that row, spanning `block` rows.
+
+    Block columns are independent, so step t takes the t-th non-zero of every
+    block column at once and tests it against that block column's starts so
+    far (the walk within a block column stays in the builder's order)."""
     rows = np.asarray(rows, np.int64)
     cols = np.asarray(cols, np.int64)
+    if rows.size == 0:
+        return 0
     idx = np.lexsort((rows, cols))
-    r_all, c_all = rows[idx].tolist(), cols[idx].tolist()
-    total, c0, starts = 0, None, []
-    for r, c in zip(r_all, c_all):
-        if c0 is None or c - c0 >= block:
-            c0, starts = c, []
-        for s0 in starts:
-            if 0 <= r - s0 < block:
-                break
-        else:
-            starts.append(r)
-            total += 1
-    return total
+    r, c = rows[idx], cols[idx]
+    # block column of every distinct column (a walk over columns, not non-zeros)
+    ucols = np.unique(c)
+    bcid = np.empty(len(ucols), np.int64)
+    c0, g = None, -1
+    for i, col in enumerate(ucols.tolist()):
+        if c0 is None or col - c0 >= block:
+            c0, g = col, g + 1
+        bcid[i] = g
+    gid = bcid[np.searchsorted(ucols, c)]
+    gstart = np.flatnonzero(np.r_[True, gid[1:] != gid[:-1]])
+    glen = np.diff(np.r_[gstart, len(r)])
+    never = np.iinfo(np.int64).min // 2  # a start that covers no row
+    starts = np.full((len(gstart), 8), never, np.int64)
+    nstart = np.zeros(len(gstart), np.int64)
+    for t in range(int(glen.max())):
+        act = np.flatnonzero(glen > t)
+        rr = r[gstart[act] + t]
+        w = int(nstart[act].max())
+        d = rr[:, None] - starts[act, :w]
+        opened = act[~((d >= 0) & (d < block)).any(axis=1)] if w else act
+        if opened.size:
+            if int(nstart[opened].max()) >= starts.shape[1]:
+                grown = np.full((len(gstart), 2 * starts.shape[1]), never, np.int64)
+                grown[:, :starts.shape[1]] = starts
+                starts = grown
+            starts[opened, nstart[opened]] = r[gstart[opened] + t]
+            nstart[opened] += 1
+    return int(nstart.sum())
 
 
 def similarity_order(rows, cols, neuron, block=BLOCK, seed=0, align=True):
@@ -150,37 +174,61 @@ def _read_layer(path, neuron):
     return np.cumsum(cp).astype(np.int32), u[idx].astype(np.int32), val[idx]
 
 
-def reorder_dataset(src, dst, neuron, layers, block=BLOCK, seed=0):
+def _reorder_file(src, dst, neuron, l, block, seed):
+    """Reads layer l of the dataset at src, writes its reordered weights under
+    dst; returns (fuse row, blocks before, blocks after)."""
+    name = os.path.join(f"neuron{neuron}", f"{neuron}-l{l + 1}.tsv")
+    cp, ri, vv = _read_layer(os.path.join(src, name), neuron)
+    order, (ncp, nri, nvv), b0, b1 = reorder_layer(cp, ri, vv, neuron, block, seed)
+    col = np.repeat(np.arange(neuron), np.diff(ncp))
+    with open(os.path.join(dst, name), "w") as f:
+        for a, b, v in zip((nri + 1).tolist(), (col + 1).tolist(), nvv.tolist()):
+            f.write(f"{a}\t{b}\t{v:.9g}\n")
+    return order, b0, b1
+
+
+def reorder_dataset(src, dst, neuron, layers, block=BLOCK, seed=0, workers=1):
     """Writes the reordered dataset (weights, images, fuse matrix) to dst;
-    returns [(blocks before, blocks after)] per layer."""
+    returns [(blocks before, blocks after)] per layer.  Layers are
+    independent: with workers > 1 they are reordered in that many processes
+    (started with spawn, so a caller that has initialised CUDA is safe); the
+    files written are the same."""
     os.makedirs(os.path.join(dst, f"neuron{neuron}"), exist_ok=True)
     os.makedirs(os.path.join(dst, "fuse_matrix", f"neuron{neuron}"), exist_ok=True)
     img = f"sparse-images-{neuron}.tsv"
     if os.path.abspath(os.path.join(src, img)) != os.path.abspath(os.path.join(dst, img)):
         shutil.copyfile(os.path.join(src, img), os.path.join(dst, img))
-    stats, fuse = [], []
-    for l in range(layers):
-        name = os.path.join(f"neuron{neuron}", f"{neuron}-l{l + 1}.tsv")
-        cp, ri, vv = _read_layer(os.path.join(src, name), neuron)
-        order, (ncp, nri, nvv), b0, b1 = reorder_layer(cp, ri, vv, neuron, block, seed)
-        col = np.repeat(np.arange(neuron), np.diff(ncp))
-        with open(os.path.join(dst, name), "w") as f:
-            for a, b, v in zip((nri + 1).tolist(), (col + 1).tolist(), nvv.tolist()):
-                f.write(f"{a}\t{b}\t{v:.9g}\n")
-        fuse.append(order)
-        stats.append((b0, b1))
+    jobs = [(src, dst, neuron, l, block, seed) for l in range(layers)]
+    if workers > 1 and layers > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=min(workers, layers), mp_context=mp.get_context("spawn")) as ex:
+            done = list(ex.map(_reorder_file, *zip(*jobs)))
+    else:
+        done = [_reorder_file(*j) for j in jobs]
     with open(os.path.join(dst, "fuse_matrix", f"neuron{neuron}", f"{neuron}_{layers}_fuse.tsv"), "w") as f:
-        for order in fuse:
+        for order, _, _ in done:
             f.write("\t".join(str(int(x)) for x in order) + "\n")
-    return stats
+    return [(b0, b1) for _, b0, b1 in done]
 
 
 def main(argv=None):
-    argv = sys.argv[1:] if argv is None else argv
+    argv = list(sys.argv[1:] if argv is None else argv)
+    workers = None
+    if "--workers" in argv:
+        i = argv.index("--workers")
+        if i + 1 >= len(argv):
+            argv = []
+        else:
+            workers = int(argv[i + 1])
+            del argv[i:i + 2]
     if len(argv) != 4:
-        print("usage: python -m cospdnn_b200.reorder SRC DST neuron layers")
+        print("usage: python -m cospdnn_b200.reorder SRC DST neuron layers [--workers N]")
         return 1
-    stats = reorder_dataset(argv[0], argv[1], int(argv[2]), int(argv[3]))
+    layers = int(argv[3])
+    if workers is None:  # one process per layer, up to the host's cores
+        workers = min(layers, os.cpu_count() or 1)
+    stats = reorder_dataset(argv[0], argv[1], int(argv[2]), layers, workers=workers)
     b0 = sum(s[0] for s in stats)
     b1 = sum(s[1] for s in stats)
     print(f"greedy 16x16 blocks: {b0} -> {b1} over {len(stats)} layers")

@@ -90,3 +90,36 @@ def test_reorder_network_and_main(oracle, tmp_path, capsys):
     f = np.loadtxt(tmp_path / "dst" / "fuse_matrix" / f"neuron{n}" / f"{n}_{L}_fuse.tsv", dtype=np.int64)
     for l in range(L):
         np.testing.assert_array_equal(f[l], fuse[l])
+
+
+def test_block_count_random_layers_with_empty_columns(oracle):
+    """The block count (block columns walked in step) equals the reference
+    builder's on random patterns, including empty columns, so that block
+    columns start off multiples of 16, and widths that are not multiples of 16."""
+    rng = np.random.default_rng(5)
+    for trial in range(120):
+        n = int(rng.choice([16, 48, 100, 256, 1000]))
+        nnz = int(rng.integers(1, 6 * n))
+        rows, cols = rng.integers(0, n, nnz), rng.integers(0, n, nnz)
+        if trial % 3 == 0:
+            cols = cols // 7 * 7
+        key = np.unique(rows * n + cols)
+        rows, cols = key // n, key % n
+        want = len(oracle.bcsc_greedy(rows, cols, np.ones(len(rows), np.float32), 16)[1])
+        assert ro.greedy_blocks(rows, cols, n) == want, trial
+    assert ro.greedy_blocks([], [], 64) == 0
+
+
+def test_parallel_layers_write_the_same_files(tmp_path):
+    from cospdnn_b200 import synth
+    n, L = 1024, 3
+    layers = [permute_rows(shift_half_block_layer(n, 13, l), n, 130 + l) for l in range(L)]
+    y0 = (np.random.default_rng(2).random((10, n)) < 0.2).astype(np.uint8)
+    synth.write_reference_dataset(str(tmp_path / "src"), n, L, y0, layers)
+    one = ro.reorder_dataset(str(tmp_path / "src"), str(tmp_path / "one"), n, L, workers=1)
+    assert ro.main([str(tmp_path / "src"), str(tmp_path / "many"), str(n), str(L), "--workers", "3"]) == 0
+    rel = [f"neuron{n}/{n}-l{l + 1}.tsv" for l in range(L)] + [f"fuse_matrix/neuron{n}/{n}_{L}_fuse.tsv"]
+    for r in rel:
+        assert (tmp_path / "one" / r).read_bytes() == (tmp_path / "many" / r).read_bytes(), r
+    assert all(b < a for a, b in one)
+    assert ro.main([str(tmp_path / "src"), str(tmp_path / "x"), str(n), "--workers"]) == 1
