@@ -32,6 +32,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -40,6 +41,7 @@
 #include <iostream>
 #include <iterator>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -66,6 +68,79 @@ inline float bias_of(int neuron) {
     }
 }
 
+// Whitespace-separated decimal numbers of a file, read in blocks (the files
+// of the 65536-neuron networks hold tens of millions of lines): integers as
+// strtol and values as strtof read them, which is what the stream
+// extraction of the reference's readers (`f >> u >> v >> val`) yields for
+// such tokens.  next() is false at the end of the file and at a token that
+// is not a number of its kind; the readers stop there, as the reference's
+// `while (f >> ...)` loops do.
+class NumReader {
+  public:
+    // block: bytes read at a time (at least twice the longest token)
+    explicit NumReader(const std::string &name, size_t block = 16u << 20)
+        : f_(std::fopen(name.c_str(), "rb")), block_(std::max(block, 2 * kToken)), buf_(block_ + 1) {}
+    ~NumReader() {
+        if (f_) std::fclose(f_);
+    }
+    NumReader(const NumReader &) = delete;
+    NumReader &operator=(const NumReader &) = delete;
+    bool ok() const { return f_ != nullptr; }
+    bool next(long &x) {
+        if (!token()) return false;
+        char *e = nullptr;
+        x = std::strtol(p_, &e, 10);
+        if (e == p_) return false;
+        p_ = e;
+        return true;
+    }
+    bool next(float &x) {
+        if (!token()) return false;
+        // decimal and exponent forms, as the stream extraction takes them:
+        // no inf or nan; "0x..." is the value 0 followed by the token "x..."
+        const char *d = p_ + (*p_ == '+' || *p_ == '-');
+        if (!((*d >= '0' && *d <= '9') || *d == '.')) return false;
+        if (d[0] == '0' && (d[1] == 'x' || d[1] == 'X')) {
+            x = *p_ == '-' ? -0.0f : 0.0f;
+            p_ = const_cast<char *>(d) + 1;
+            return true;
+        }
+        char *e = nullptr;
+        x = std::strtof(p_, &e);
+        if (e == p_) return false;
+        // an exponent without digits ("1e", "1e+") fails the stream extraction
+        if ((*e == 'e' || *e == 'E') && std::find_if(p_, e, [](char ch) { return ch == 'e' || ch == 'E'; }) == e)
+            return false;
+        p_ = e;
+        return true;
+    }
+
+  private:
+    static constexpr size_t kToken = 4096;  // longest token read whole
+    // skips white space; true when a token starts at p_ with at least kToken
+    // bytes (or the rest of the file) behind it in the buffer
+    bool token() {
+        for (;;) {
+            while (p_ < end_ && (*p_ == ' ' || *p_ == '\t' || *p_ == '\n' || *p_ == '\r' || *p_ == '\v' ||
+                                 *p_ == '\f'))
+                ++p_;
+            if (eof_ || (size_t)(end_ - p_) >= kToken) return p_ < end_;
+            const size_t keep = (size_t)(end_ - p_);
+            if (keep) std::memmove(buf_.data(), p_, keep);
+            const size_t got = f_ ? std::fread(buf_.data() + keep, 1, block_ - keep, f_) : 0;
+            eof_ = got < block_ - keep;
+            p_ = buf_.data();
+            end_ = p_ + keep + got;
+            *end_ = '\0';  // strtol/strtof stop here
+        }
+    }
+    std::FILE *f_;
+    size_t block_;
+    std::vector<char> buf_;
+    char *p_ = nullptr, *end_ = nullptr;
+    bool eof_ = false;
+};
+
 // Dense rows [batch][neuron]; `integral` stays true while every value is an
 // integer in 0..255 (then the rows are handed over as bytes).
 struct Input {
@@ -74,40 +149,41 @@ struct Input {
     long read = 0;
 };
 
-inline Input read_input(int neuron, int batch, const std::string &dir) {
+// Reads the images into in; returns "" or what is wrong with the file (read
+// on its own thread while the layers are parsed, the caller reports it).
+inline std::string read_input(int neuron, int batch, const std::string &dir, Input &in) {
     const std::string name = dir + "/sparse-images-" + std::to_string(neuron) + ".tsv";
-    std::ifstream f(name);
-    if (!f) die("FILE:" + name + " does not exists.");
-    Input in;
+    NumReader f(name);
+    if (!f.ok()) return "FILE:" + name + " does not exists.";
+    in = Input();
     in.rows.assign((size_t)batch * neuron, 0.0f);
     long b, n;
     float val;
-    while (f >> b >> n >> val) {
+    while (f.next(b) && f.next(n) && f.next(val)) {
         if (b < 1 || b > batch) continue;
-        if (n < 1 || n > neuron) die("input neuron index out of range in " + name);
+        if (n < 1 || n > neuron) return "input neuron index out of range in " + name;
         in.rows[(size_t)(b - 1) * neuron + (n - 1)] = val;
         if (!(val >= 0.0f && val <= 255.0f && (float)(int)val == val)) in.integral = false;
         ++in.read;
     }
-    std::cout << "Read Input success! read_numeber = " << in.read << std::endl;
-    return in;
+    return "";
 }
 
-inline std::vector<std::vector<int32_t>> read_fuse(int neuron, int layers, const std::string &dir) {
+// Reads the fuse rows of every layer; returns "" or what is wrong with the file.
+inline std::string read_fuse(int neuron, int layers, const std::string &dir, std::vector<std::vector<int32_t>> &fuse) {
     const std::string name = dir + "/fuse_matrix/neuron" + std::to_string(neuron) + "/" + std::to_string(neuron) +
                              "_" + std::to_string(layers) + "_fuse.tsv";
-    std::ifstream f(name);
-    if (!f) die("FILE:" + name + " does not exists.");
-    std::vector<std::vector<int32_t>> fuse(layers, std::vector<int32_t>(neuron));
+    NumReader f(name);
+    if (!f.ok()) return "FILE:" + name + " does not exists.";
+    fuse.assign(layers, std::vector<int32_t>(neuron));
     for (int l = 0; l < layers; ++l)
         for (int j = 0; j < neuron; ++j) {
             float t;
-            if (!(f >> t)) die(" read error");
+            if (!f.next(t)) return " read error";
             fuse[l][j] = (int32_t)t;
-            if (fuse[l][j] < 0 || fuse[l][j] >= neuron) die("fuse entry out of range in " + name);
+            if (fuse[l][j] < 0 || fuse[l][j] >= neuron) return "fuse entry out of range in " + name;
         }
-    std::cout << "Read fuse success!" << std::endl;
-    return fuse;
+    return "";
 }
 
 // One layer as CSC over (activation row, output), fuse applied, duplicates summed.
@@ -116,19 +192,21 @@ struct Csc {
     std::vector<float> vals;
 };
 
-inline Csc read_layer(int neuron, int l, const std::vector<int32_t> &fuse, const std::string &dir) {
+// Reads layer l into c; returns "" or the message of what is wrong with the
+// file (layers are read on several threads, the caller reports it).
+inline std::string read_layer(int neuron, int l, const std::vector<int32_t> &fuse, const std::string &dir, Csc &c) {
     const std::string name =
         dir + "/neuron" + std::to_string(neuron) + "/" + std::to_string(neuron) + "-l" + std::to_string(l + 1) + ".tsv";
-    std::ifstream f(name);
-    if (!f) die("File:" + name + " does not exists.");
+    NumReader f(name);
+    if (!f.ok()) return "File:" + name + " does not exists.";
     std::vector<std::vector<std::pair<int32_t, float>>> cols(neuron);
     long u, v;
     float val;
-    while (f >> u >> v >> val) {
-        if (u < 1 || u > neuron || v < 1 || v > neuron) die("weight index out of range in " + name);
+    while (f.next(u) && f.next(v) && f.next(val)) {
+        if (u < 1 || u > neuron || v < 1 || v > neuron) return "weight index out of range in " + name;
         cols[v - 1].push_back({fuse[u - 1], val});
     }
-    Csc c;
+    c = Csc();
     c.colptr.assign(neuron + 1, 0);
     for (int j = 0; j < neuron; ++j) {
         auto &e = cols[j];
@@ -143,7 +221,7 @@ inline Csc read_layer(int neuron, int l, const std::vector<int32_t> &fuse, const
         }
         c.colptr[j + 1] = (int32_t)c.rowidx.size();
     }
-    return c;
+    return "";
 }
 
 // One network as the engine sees it.
@@ -170,9 +248,32 @@ inline Network parse_network(int neuron, int batch, int layers, const std::strin
     n.neuron = neuron;
     n.batch = batch;
     n.layers = layers;
-    n.input = read_input(neuron, batch, dir);
-    const auto fuse = read_fuse(neuron, layers, dir);
-    for (int l = 0; l < layers; ++l) n.w.push_back(read_layer(neuron, l, fuse[l], dir));
+    // the images on one thread; the fuse, then the layer files (independent)
+    // on one thread per core; messages in file order once all are read
+    std::string ein, efuse;
+    std::thread tin([&] { ein = read_input(neuron, batch, dir, n.input); });
+    std::vector<std::vector<int32_t>> fuse;
+    efuse = read_fuse(neuron, layers, dir, fuse);
+    n.w.resize(layers);
+    std::vector<std::string> err(layers);
+    if (efuse.empty()) {
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (int l; (l = next++) < layers;) err[l] = read_layer(neuron, l, fuse[l], dir, n.w[l]);
+        };
+        const int nt = std::max(1, std::min(layers, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (auto &t : pool) t.join();
+    }
+    tin.join();
+    if (!ein.empty()) die(ein);
+    std::cout << "Read Input success! read_numeber = " << n.input.read << std::endl;
+    if (!efuse.empty()) die(efuse);
+    std::cout << "Read fuse success!" << std::endl;
+    for (int l = 0; l < layers; ++l)
+        if (!err[l].empty()) die(err[l]);
     return n;
 }
 

@@ -1,5 +1,7 @@
-"""Host-side parts of the command lines, on CPU: the binary dataset cache
-(COSPDNN_CACHE) and the categories files (COSPDNN_CATEGORIES, COSPDNN_TRUTH),
+"""Host-side parts of the command lines, on CPU: the number reader of the
+dataset files (the same numbers as the reference's stream extraction), the
+binary dataset cache (COSPDNN_CACHE) and the categories files
+(COSPDNN_CATEGORIES, COSPDNN_TRUTH),
 through a small program built with g++ against cospdnn_b200/cli/reference_io.h,
 and the Python categories module (cospdnn_b200.categories)."""
 import os
@@ -33,8 +35,30 @@ static uint64_t digest(const Network &n) {
     }
     return h;
 }
+// (u, v, val) triples until the first that does not parse, as the stream
+// extraction reads them and as NumReader reads them with `block`-byte reads
+static void triples(const char *path, size_t block) {
+    uint64_t hs = 1469598103934665603ull, hr = hs;
+    long ns = 0, nr = 0, u, v;
+    float val;
+    std::ifstream f(path);
+    while (f >> u >> v >> val) {
+        hs = mix(mix(mix(hs, &u, sizeof u), &v, sizeof v), &val, sizeof val);
+        ++ns;
+    }
+    NumReader r(path, block);
+    while (r.next(u) && r.next(v) && r.next(val)) {
+        hr = mix(mix(mix(hr, &u, sizeof u), &v, sizeof v), &val, sizeof val);
+        ++nr;
+    }
+    printf("stream %" PRIu64 " %ld\nreader %" PRIu64 " %ld\n", hs, ns, hr, nr);
+}
 int main(int argc, char **argv) {
     const std::string mode = argv[1];
+    if (mode == "nums") {
+        triples(argv[2], (size_t)atol(argv[3]));
+        return 0;
+    }
     if (mode == "load" || mode == "parse") {
         const int n = atoi(argv[2]), b = atoi(argv[3]), l = atoi(argv[4]);
         const Network net = mode == "load" ? load_network(n, b, l, argv[5]) : parse_network(n, b, l, argv[5]);
@@ -59,7 +83,7 @@ def harness(tmp_path_factory):
     src.write_text(HARNESS)
     exe = d / "h"
     subprocess.run([gxx, "-O1", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), "-I",
-                    os.path.join(ROOT, "cospdnn_b200", "cli"), str(src), "-o", str(exe)], check=True)
+                    os.path.join(ROOT, "cospdnn_b200", "cli"), str(src), "-o", str(exe), "-pthread"], check=True)
     return str(exe)
 
 
@@ -168,3 +192,49 @@ def test_categories_module(tmp_path):
     bad.write_text("0\n")
     with pytest.raises(ValueError):
         cat.read(bad)
+
+
+def _fmt_triples(rng, n):
+    """Lines of "u v val" with mixed white space and number forms."""
+    ws = [" ", "\t", "  ", " \t ", "\t\t"]
+    ends = ["\n", "\r\n", " \n", "\n\n", "\t\n"]
+    out = []
+    for _ in range(n):
+        u, v = int(rng.integers(1, 5000)), int(rng.integers(1, 5000))
+        val = float(rng.choice([0.0625, -0.25, 1.0, 3.0, 1e-5, 2.5e7]) * rng.choice([1, -1]))
+        form = int(rng.integers(0, 6))
+        txt = [f"{val}", f"{val:.9g}", f"{val:e}", f"{val:E}", f"{val:.3f}", f"+{abs(val)}"][form]
+        if form == 4 and abs(val) < 1 and txt.startswith("0"):
+            txt = txt[1:]  # ".062"
+        us = f"+{u}" if rng.random() < 0.05 else str(u)
+        out.append(us + rng.choice(ws) + str(v) + rng.choice(ws) + txt + rng.choice(ends))
+    return out
+
+
+@pytest.mark.parametrize("bad", [None, "abc", "1e", "1e+", "0x5", "-0x1p3", "inf", "nan", "5e3e2", "--3", "+.",
+                                 ".", "7.5.3", "1.5e"])
+def test_number_reader_matches_stream_extraction(harness, tmp_path, bad):
+    """NumReader stops where `while (f >> u >> v >> val)` stops and reads the
+    same numbers, across many 8 KB reads (tokens split between reads) and
+    with a malformed token in the value or index position."""
+    rng = np.random.default_rng(0 if bad is None else len(bad) * 7 + ord(bad[0]))
+    lines = _fmt_triples(rng, 20000)
+    if bad is not None:
+        at = int(rng.integers(100, 19000))
+        parts = lines[at].split()
+        parts[int(rng.integers(0, 3))] = bad
+        lines[at] = " ".join(parts) + "\n"
+    path = tmp_path / "t.tsv"
+    path.write_text("".join(lines).rstrip("\n"))  # no newline at the end
+    for block in (8192, 1 << 24):
+        rc, out = _run(harness, ["nums", path, block])
+        got = dict(line.split(" ", 1) for line in out.strip().splitlines())
+        assert rc == 0 and got["stream"] == got["reader"], (bad, block, got)
+        if bad is None:
+            assert got["reader"].split()[1] == "20000"
+    for text in ("", "  \n\t\n", "1 2 0.5"):
+        path.write_text(text)
+        rc, out = _run(harness, ["nums", path, 8192])
+        got = dict(line.split(" ", 1) for line in out.strip().splitlines())
+        assert got["stream"] == got["reader"], text
+
