@@ -123,3 +123,14 @@ def test_parallel_layers_write_the_same_files(tmp_path):
         assert (tmp_path / "one" / r).read_bytes() == (tmp_path / "many" / r).read_bytes(), r
     assert all(b < a for a, b in one)
     assert ro.main([str(tmp_path / "src"), str(tmp_path / "x"), str(n), "--workers"]) == 1
+
+
+@pytest.mark.parametrize("name", ["bcsc_r1_n256", "bcsc_rand_n80_gaps", "bcsc_rand_n96", "bcsc_xor_n128_m32",
+                                  "bcsc_xor_n256_m32", "bcsc_xor_n64_bs8", "bcsc_xor_n64_m8"])
+def test_block_count_matches_reference_builder_fixtures(name):
+    """The block count equals the number of blocks the reference's own
+    builder (compiled from its sources) made for the golden fixtures."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+    n = int(max(g["row"].max(), g["col"].max())) + 1
+    assert ro.greedy_blocks(g["row"], g["col"], n, int(g["bs"])) == len(g["row_index"])
