@@ -39,6 +39,7 @@ int main(int argc, char *argv[]) {
         devices.push_back(dev);
     } else {
         const int avail = cospdnn_device_count();
+        if (avail < 1) die("no CUDA device visible");
         if (gpu_num > avail) {
             std::cout << "Exceeding Maximum GPU Number! Automatically Change to Max GPU Number " << avail << std::endl;
             gpu_num = avail;

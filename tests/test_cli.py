@@ -30,6 +30,19 @@ def test_cli_usage(name, nargs):
     assert out.stdout.startswith("Usage: exe neuron")
 
 
+@pytest.mark.parametrize("gpu_num", [1, 2])
+def test_cli_fails_without_a_device(tmp_path, gpu_num):
+    """With no CUDA device visible the program exits with an error for one
+    GPU and for several (it does not report an empty result)."""
+    from cospdnn_b200 import synth
+    csc, y0, _ = make_net(64, 2, 10, seed=1, dlo=0.2, dhi=0.4)
+    synth.write_reference_dataset(str(tmp_path), 64, 2, y0, csc)
+    out = subprocess.run([_exe("cospdnn"), "64", "10", "2", str(gpu_num), "0", str(tmp_path)], capture_output=True,
+                         text=True, timeout=120, env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert out.returncode != 0
+    assert "Kernel Exec Time" not in out.stdout and "[Categories]" not in out.stdout
+
+
 def _dataset(tmp, n, L, rows, seed, net):
     """Writes a net in the reference's formats with a random fuse per layer and
     returns the oracle's view (weights folded through the fuse)."""
