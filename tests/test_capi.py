@@ -61,3 +61,22 @@ def test_run_networks_rejects_bad_arguments_without_gpu():
     net.desc.neuron, net.desc.layers, net.desc.rows = 64, 1, 10
     assert L.cospdnn_run_networks(C.addressof(net), 1, 0, None) == cs.ERR_INVALID
     assert b"run_networks" in L.cospdnn_last_error()
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/cospdnn_b200.h compiles as C99 (no C++ in the boundary) and a C
+    program links against the library and calls it."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    libdir = os.path.join(ROOT, "cospdnn_b200")
+    if gcc is None or not os.path.exists(os.path.join(libdir, "libcospdnn_b200.so")):
+        pytest.skip("gcc or the built library missing")
+    src = tmp_path / "c.c"
+    src.write_text('#include "cospdnn_b200.h"\n'
+                   'int main(void) { return cospdnn_version() >= 100 && cospdnn_last_error() ? 0 : 1; }\n')
+    exe = tmp_path / "c"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", libdir, "-lcospdnn_b200", f"-Wl,-rpath,{libdir}"], check=True,
+                   timeout=120)
+    assert subprocess.run([str(exe)], timeout=60).returncode == 0
