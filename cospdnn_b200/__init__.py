@@ -319,3 +319,54 @@ def test_graph_challenge_tc(input, weight, row_idx, ptr, fuse_list, batch, neuro
             print(f"layer {l}, feature = {n}")
     res["categories"] = res["categories"] + lo
     return res
+
+
+def test_graph_challenge_tc_co(input1, weight1, row_idx1, ptr1, fuse_list1, batch1, neuron1, bias1,
+                               input2, weight2, row_idx2, ptr2, fuse_list2, batch2, neuron2, bias2,
+                               blocksize_c=16, blocksize_r=16, gpu_id=0, gpu_num=1,
+                               precision=PREC_FP16, threshold=THRESHOLD, verbose=True):
+    """Mirror of the reference's test_graph_challenge_tc_co
+    (src/cospdnn_double.cu:208-1214): two networks, each given as in
+    test_graph_challenge_tc, run in one engine and one graph launch.  They may
+    differ in width, depth and batch (the reference needs equal depth).  Each
+    network's rows are split over gpu_num slices and slice gpu_id is computed,
+    as in src/cospdnn_double.cu:236-274.  Prints "SpDNN k layer l, feature = n"
+    for network k = 1, 2 when verbose and returns one dict(categories, alive)
+    per network.  Raises on error instead of exiting."""
+    if blocksize_c != blocksize_r:
+        raise CospdnnError(ERR_UNSUPPORTED, "square blocks only")
+    nets = ((input1, weight1, row_idx1, ptr1, fuse_list1, batch1, neuron1, bias1),
+            (input2, weight2, row_idx2, ptr2, fuse_list2, batch2, neuron2, bias2))
+    eng = Engine(gpu_id if gpu_num > 1 else 0)
+    ids, los, xs = [], [], []
+    try:
+        for inp, weight, row_idx, ptr, fuse_list, batch, neuron, bias in nets:
+            rows_per = (batch + gpu_num - 1) // gpu_num
+            lo, hi = gpu_id * rows_per, min((gpu_id + 1) * rows_per, batch)
+            nid = eng.add_net(neuron, len(weight), hi - lo, bias, threshold, precision)
+            for l in range(len(weight)):
+                fz = None if fuse_list is None else fuse_list[l]
+                eng.set_layer_bcsc(nid, l, ptr[l], row_idx[l], weight[l], blocksize_c, fz)
+            ids.append(nid)
+            los.append(lo)
+            xs.append(np.asarray(inp)[lo:hi])
+        eng.build()
+        for nid, x in zip(ids, xs):
+            eng.set_input(nid, x.astype(np.uint8) if np.all((x == 0) | (x == 1)) else x.astype(np.float32))
+        eng.run()
+        res = [eng.result(nid) for nid in ids]
+    finally:
+        eng.close()
+    for k, (r, lo) in enumerate(zip(res, los)):
+        if verbose:
+            for l, n in enumerate(r["alive"]):
+                print(f"SpDNN {k + 1} layer {l}, feature = {n}")
+        r["categories"] = r["categories"] + lo
+    return res[0], res[1]
+
+
+# mirrors of the reference's host functions, not tests (pytest collects names
+# that start with "test" from a module that imports them)
+test_graph_challenge_tc.__test__ = False
+test_graph_challenge_tc_co.__test__ = False
+
