@@ -433,14 +433,34 @@ int colour_group(int P, const std::vector<int> &eu, const std::vector<int> &es, 
     }
     int D = 0;
     for (int v = 0; v < P; ++v) D = std::max(D, std::max(du[v], ds[v]));
+    // edge of each (vertex, colour) and, per vertex, a bit mask of its used
+    // colours (the lowest free colour is the lowest clear bit)
+    const int W = (D + 63) / 64;
     std::vector<int> atU((size_t)P * D, -1), atS((size_t)P * D, -1);
+    std::vector<uint64_t> mU((size_t)P * W, 0), mS((size_t)P * W, 0);
+    auto put = [&](int f, int c) {
+        atU[(size_t)eu[f] * D + c] = f;
+        atS[(size_t)es[f] * D + c] = f;
+        mU[(size_t)eu[f] * W + c / 64] |= 1ull << (c % 64);
+        mS[(size_t)es[f] * W + c / 64] |= 1ull << (c % 64);
+    };
+    auto take = [&](int f, int c) {
+        atU[(size_t)eu[f] * D + c] = -1;
+        atS[(size_t)es[f] * D + c] = -1;
+        mU[(size_t)eu[f] * W + c / 64] &= ~(1ull << (c % 64));
+        mS[(size_t)es[f] * W + c / 64] &= ~(1ull << (c % 64));
+    };
+    // a vertex with an uncoloured edge has a free colour below D
+    auto lowest_free = [&](const std::vector<uint64_t> &m, int v) {
+        int w = 0;
+        while (m[(size_t)v * W + w] == ~0ull) ++w;
+        return w * 64 + __builtin_ctzll(~m[(size_t)v * W + w]);
+    };
     colour.assign(E, -1);
     std::vector<int> path;
     for (int e = 0; e < E; ++e) {
         const int u = eu[e], s = es[e];
-        int a = 0, b = 0;
-        while (atU[(size_t)u * D + a] >= 0) ++a;
-        while (atS[(size_t)s * D + b] >= 0) ++b;
+        const int a = lowest_free(mU, u), b = lowest_free(mS, s);
         if (atS[(size_t)s * D + a] >= 0) {
             // a/b path from s, starting with the edge of colour a
             path.clear();
@@ -454,19 +474,14 @@ int colour_group(int P, const std::vector<int> &eu, const std::vector<int> &es, 
                 onS = !onS;
                 cc = cc == a ? b : a;
             }
-            for (int f : path) {
-                atU[(size_t)eu[f] * D + colour[f]] = -1;
-                atS[(size_t)es[f] * D + colour[f]] = -1;
-            }
+            for (int f : path) take(f, colour[f]);
             for (int f : path) {
                 colour[f] = colour[f] == a ? b : a;
-                atU[(size_t)eu[f] * D + colour[f]] = f;
-                atS[(size_t)es[f] * D + colour[f]] = f;
+                put(f, colour[f]);
             }
         }
         colour[e] = a;
-        atU[(size_t)u * D + a] = e;
-        atS[(size_t)s * D + a] = e;
+        put(e, a);
     }
     return D;
 }
