@@ -43,6 +43,20 @@ def test_cli_fails_without_a_device(tmp_path, gpu_num):
     assert "Kernel Exec Time" not in out.stdout and "[Categories]" not in out.stdout
 
 
+def test_cli_writes_cache_before_it_needs_a_device(tmp_path):
+    """The dataset is parsed and cached before the first CUDA call, so a run
+    on a host without a GPU prepares the cache (and then stops with an error)."""
+    from cospdnn_b200 import synth
+    csc, y0, _ = make_net(64, 2, 10, seed=2, dlo=0.2, dhi=0.4)
+    synth.write_reference_dataset(str(tmp_path / "d"), 64, 2, y0, csc)
+    (tmp_path / "c").mkdir()
+    out = subprocess.run([_exe("cospdnn"), "64", "10", "2", "1", "0", str(tmp_path / "d")], capture_output=True,
+                         text=True, timeout=120,
+                         env=dict(os.environ, CUDA_VISIBLE_DEVICES="", COSPDNN_CACHE=str(tmp_path / "c")))
+    assert out.returncode != 0
+    assert (tmp_path / "c" / "cospdnn-n64-b10-l2.bin").stat().st_size > 0
+
+
 def _dataset(tmp, n, L, rows, seed, net):
     """Writes a net in the reference's formats with a random fuse per layer and
     returns the oracle's view (weights folded through the fuse)."""
