@@ -57,6 +57,42 @@ def test_cli_writes_cache_before_it_needs_a_device(tmp_path):
     assert (tmp_path / "c" / "cospdnn-n64-b10-l2.bin").stat().st_size > 0
 
 
+@pytest.mark.parametrize("fault,message", [
+    ("no_images", "sparse-images-64.tsv does not exists."),
+    ("no_layer", "64-l2.tsv does not exists."),
+    ("weight_index", "weight index out of range in"),
+    ("fuse_entry", "fuse entry out of range in"),
+    ("fuse_short", "read error"),
+    ("image_neuron", "input neuron index out of range in"),
+])
+def test_cli_bad_dataset_files(tmp_path, fault, message):
+    """Damaged dataset files end the run with the reference's kind of message
+    and a non-zero exit status, before any device is needed."""
+    from cospdnn_b200 import synth
+    csc, y0, _ = make_net(64, 2, 10, seed=3, dlo=0.2, dhi=0.4)
+    d = tmp_path / "d"
+    synth.write_reference_dataset(str(d), 64, 2, y0, csc)
+    fuse = d / "fuse_matrix" / "neuron64" / "64_2_fuse.tsv"
+    if fault == "no_images":
+        (d / "sparse-images-64.tsv").unlink()
+    elif fault == "no_layer":
+        (d / "neuron64" / "64-l2.tsv").unlink()
+    elif fault == "weight_index":
+        with open(d / "neuron64" / "64-l1.tsv", "a") as f:
+            f.write("65\t1\t0.0625\n")
+    elif fault == "fuse_entry":
+        fuse.write_text("64 " + fuse.read_text())
+    elif fault == "fuse_short":
+        fuse.write_text(fuse.read_text().split("\n")[0] + "\n")
+    else:
+        with open(d / "sparse-images-64.tsv", "a") as f:
+            f.write("1\t65\t1\n")
+    out = subprocess.run([_exe("cospdnn"), "64", "10", "2", "1", "0", str(d)], capture_output=True, text=True,
+                         timeout=120, env=dict(os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert out.returncode != 0
+    assert message in out.stdout, out.stdout
+
+
 def _dataset(tmp, n, L, rows, seed, net):
     """Writes a net in the reference's formats with a random fuse per layer and
     returns the oracle's view (weights folded through the fuse)."""
