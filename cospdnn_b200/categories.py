@@ -5,8 +5,11 @@ the last layer, as 1-based ids, one per line, ascending -- the format of the
 challenge's truth files.  The engine returns 0-based rows.
 
     python -m cospdnn_b200.categories OURS TRUTH
+    python -m cospdnn_b200.categories --hash FILE
 
-compares two such files and exits 0 when they hold the same ids, 2 if not.
+compares two such files and exits 0 when they hold the same ids, 2 if not;
+--hash prints the FNV-1a (64-bit) hash of the file's ids in that format, the
+`category_hash` of the command lines' COSPDNN_JSON result line.
 """
 import sys
 
@@ -34,6 +37,16 @@ def read(path):
     return np.unique(np.asarray(ids, np.int64))
 
 
+def digest(rows0):
+    """FNV-1a (64-bit) of the categories file these 0-based rows make (the
+    bytes of write()), as 16 hex digits."""
+    h = 0xCBF29CE484222325  # FNV-1a offset basis; prime 2^40 + 2^8 + 0xb3
+    for v in (np.unique(np.asarray(rows0, np.int64)) + 1).tolist():
+        for ch in f"{v}\n".encode():
+            h = ((h ^ ch) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return f"{h:016x}"
+
+
 def check(rows0, truth_path):
     """Compares 0-based rows with a truth file: dict(ok, ours, truth,
     missing, extra) where missing/extra are 0-based rows."""
@@ -47,8 +60,11 @@ def check(rows0, truth_path):
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
+    if len(argv) == 2 and argv[0] == "--hash":
+        print(f"fnv1a64:{digest(read(argv[1]))}")
+        return 0
     if len(argv) != 2:
-        print("usage: python -m cospdnn_b200.categories OURS TRUTH")
+        print("usage: python -m cospdnn_b200.categories OURS TRUTH | --hash FILE")
         return 1
     r = check(read(argv[0]), argv[1])
     print(f"categories check: {'PASS' if r['ok'] else 'FAIL'} (ours {r['ours']}, truth {r['truth']}, "

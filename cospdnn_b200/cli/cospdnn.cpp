@@ -9,7 +9,9 @@
 // are summed.  COSPDNN_PRECISION / COSPDNN_KERNEL select precision and kernel;
 // COSPDNN_CACHE keeps parsed datasets in binary form; COSPDNN_CATEGORIES /
 // COSPDNN_TRUTH write the categories in Graph Challenge format and check them
-// against a truth file (exit status 2 on a mismatch).  See reference_io.h.
+// against a truth file (exit status 2 on a mismatch); COSPDNN_JSON=1 (or a
+// file name) adds one JSON result line (edges/s, rows alive and rechecked
+// per layer, category count and hash).  See reference_io.h.
 #include <algorithm>
 #include <thread>
 
@@ -47,7 +49,7 @@ int main(int argc, char *argv[]) {
         for (int g = 0; g < gpu_num; ++g) devices.push_back(g);
     }
     const int ng = (int)devices.size();
-    std::vector<std::vector<int64_t>> alive(ng, std::vector<int64_t>(layers, 0));
+    std::vector<std::vector<int64_t>> alive(ng, std::vector<int64_t>(layers, 0)), rech(alive);
     std::vector<int64_t> count(ng, 0);
     std::vector<std::vector<int32_t>> cats(ng);
     std::vector<float> ms(ng, 0.0f);
@@ -62,7 +64,8 @@ int main(int argc, char *argv[]) {
         set_rows(e, id, net, r0, r1);
         check(cospdnn_engine_run_timed(e, nullptr, &ms[g]), "run");
         cats[g].assign((size_t)std::max(1, r1 - r0), 0);
-        check(cospdnn_engine_result(e, id, cats[g].data(), &count[g], alive[g].data(), nullptr, nullptr), "result");
+        check(cospdnn_engine_result(e, id, cats[g].data(), &count[g], alive[g].data(), rech[g].data(), nullptr),
+              "result");
         cats[g].resize((size_t)count[g]);
         for (auto &c : cats[g]) c += r0;  // rows of the whole batch
         cospdnn_engine_destroy(e);
@@ -90,6 +93,25 @@ int main(int argc, char *argv[]) {
     std::vector<int64_t> all;
     for (int g = 0; g < ng; ++g) all.insert(all.end(), cats[g].begin(), cats[g].end());
     const int rc = report_categories(all, "COSPDNN_CATEGORIES", "COSPDNN_TRUTH", "");
+    RunReport rep;
+    rep.program = "cospdnn";
+    rep.neuron = neuron;
+    rep.batch = batch;
+    rep.layers = layers;
+    rep.precision = prec;
+    rep.kernel = kern;
+    rep.gpus = ng;
+    for (const auto &w : net.w) rep.weights += (int64_t)w.rowidx.size();
+    rep.ms = tmax;
+    rep.alive.assign(layers, 0);
+    rep.rechecked.assign(layers, 0);
+    for (int g = 0; g < ng; ++g)
+        for (int l = 0; l < layers; ++l) {
+            rep.alive[l] += alive[g][l];
+            rep.rechecked[l] += rech[g][l];
+        }
+    rep.categories = all;
+    report_json(rep);
     std::cout << "Kernel Exec Time = " << tmax << "ms" << std::endl;
     std::cout << "[END]..." << std::endl;
     return rc;

@@ -5,8 +5,9 @@
 // may differ in width, depth and batch).  Prints the reference's lines
 // "SpDNN 1 layer l, feature = n", "SpDNN 2 layer l, feature = n" and
 // "Total Kernel Exec Time = X ms".  COSPDNN_PRECISION / COSPDNN_KERNEL select
-// precision and kernel; COSPDNN_CACHE, COSPDNN_CATEGORIES_1/_2 and
-// COSPDNN_TRUTH_1/_2 as in cospdnn.out (exit status 2 on a mismatch).
+// precision and kernel; COSPDNN_CACHE, COSPDNN_CATEGORIES_1/_2,
+// COSPDNN_TRUTH_1/_2 (exit status 2 on a mismatch) and COSPDNN_JSON (one
+// result line per network, timed over the joint run) as in cospdnn.out.
 #include "reference_io.h"
 
 using namespace cospdnn_cli;
@@ -44,10 +45,10 @@ int main(int argc, char *argv[]) {
     check(cospdnn_engine_run_timed(e, nullptr, &ms), "run");
     int rc = 0;
     for (int i = 0; i < 2; ++i) {
-        std::vector<int64_t> alive(layers[i], 0);
+        std::vector<int64_t> alive(layers[i], 0), rech(layers[i], 0);
         std::vector<int32_t> cats((size_t)batch[i], 0);
         int64_t count = 0;
-        check(cospdnn_engine_result(e, id[i], cats.data(), &count, alive.data(), nullptr, nullptr), "result");
+        check(cospdnn_engine_result(e, id[i], cats.data(), &count, alive.data(), rech.data(), nullptr), "result");
         for (int l = 0; l < layers[i]; ++l)
             std::cout << "SpDNN " << i + 1 << " layer " << l << ", feature = " << alive[l] << std::endl;
         std::cout << "[Categories" << i + 1 << "] :" << count << std::endl;
@@ -55,6 +56,20 @@ int main(int argc, char *argv[]) {
         const std::string k = std::to_string(i + 1);
         rc = std::max(rc, report_categories(c64, ("COSPDNN_CATEGORIES_" + k).c_str(), ("COSPDNN_TRUTH_" + k).c_str(),
                                             "SpDNN " + k + " "));
+        RunReport rep;
+        rep.program = "cospdnn_double";
+        rep.network = i + 1;
+        rep.neuron = neuron[i];
+        rep.batch = batch[i];
+        rep.layers = layers[i];
+        rep.precision = prec;
+        rep.kernel = kern;
+        for (const auto &w : net[i].w) rep.weights += (int64_t)w.rowidx.size();
+        rep.ms = ms;  // both networks run in one launch
+        rep.alive = alive;
+        rep.rechecked = rech;
+        rep.categories = c64;
+        report_json(rep);
     }
     cospdnn_engine_destroy(e);
     std::cout << "Total Kernel Exec Time = " << ms << "ms" << std::endl;

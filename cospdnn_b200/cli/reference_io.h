@@ -502,6 +502,76 @@ inline void set_rows(cospdnn_engine *e, int id, const Network &net, int r0, int 
 
 // Precision and kernel from the environment (COSPDNN_PRECISION = fp32 | fp16
 // | bf16, default fp16; COSPDNN_KERNEL = auto | cuda-core | tcgen05).
+// FNV-1a (64-bit) of the categories file these rows make (Graph Challenge
+// format: 1-based ids, one per line, ascending), so that a run can be compared
+// with a truth file by its hash (cospdnn_b200.categories computes the same).
+inline uint64_t categories_hash(const std::vector<int64_t> &cats0) {
+    std::vector<int64_t> c(cats0);
+    std::sort(c.begin(), c.end());
+    c.erase(std::unique(c.begin(), c.end()), c.end());
+    uint64_t h = 0xcbf29ce484222325ull;  // FNV-1a offset basis; prime 2^40 + 2^8 + 0xb3
+    for (int64_t r : c) {
+        const std::string line = std::to_string(r + 1) + "\n";
+        for (unsigned char ch : line) h = (h ^ ch) * 1099511628211ull;
+    }
+    return h;
+}
+
+// What a run reports in its JSON result line.
+struct RunReport {
+    std::string program;
+    int network = 0;  // 1 or 2 in the two-network program, else 0
+    int neuron = 0, batch = 0, layers = 0, precision = COSPDNN_PREC_FP16, kernel = COSPDNN_KERNEL_AUTO, gpus = 1;
+    int64_t weights = 0;  // non-zeros over all layers
+    float ms = 0.0f;      // device time of the run (max over GPUs)
+    std::vector<int64_t> alive, rechecked, categories;
+};
+
+// The result line: sizes, device time, edges = rows x non-zeros of every
+// layer and edges/s, rows alive and rows re-decided in FP64 per layer, the
+// number of categories and their hash.
+inline std::string json_line(const RunReport &r) {
+    static const char *prec[] = {"fp32", "fp16", "bf16"};
+    static const char *kern[] = {"auto", "cuda-core", "tcgen05"};
+    auto list = [](const std::vector<int64_t> &v) {
+        std::string t = "[";
+        for (size_t i = 0; i < v.size(); ++i) t += (i ? "," : "") + std::to_string(v[i]);
+        return t + "]";
+    };
+    const double edges = (double)r.batch * (double)r.weights;
+    char num[160];
+    std::snprintf(num, sizeof num, "\"ms\": %.6g, \"edges\": %.17g, \"edges_per_s\": %.6g", (double)r.ms, edges,
+                  r.ms > 0.0f ? edges / (r.ms * 1e-3) : 0.0);
+    char hash[40];
+    std::snprintf(hash, sizeof hash, "%016llx", (unsigned long long)categories_hash(r.categories));
+    std::string j = "{\"program\": \"" + r.program + "\"";
+    if (r.network) j += ", \"network\": " + std::to_string(r.network);
+    j += ", \"neuron\": " + std::to_string(r.neuron) + ", \"batch\": " + std::to_string(r.batch) +
+         ", \"layers\": " + std::to_string(r.layers) + ", \"precision\": \"" +
+         prec[std::min(std::max(r.precision, 0), 2)] + "\", \"kernel\": \"" + kern[std::min(std::max(r.kernel, 0), 2)] +
+         "\", \"gpus\": " + std::to_string(r.gpus) + ", \"weights\": " + std::to_string(r.weights) + ", " + num +
+         ", \"alive\": " + list(r.alive) + ", \"fp64_rechecked\": " + list(r.rechecked) +
+         ", \"categories\": " + std::to_string(r.categories.size()) + ", \"category_hash\": \"fnv1a64:" + hash +
+         "\"}";
+    return j;
+}
+
+// COSPDNN_JSON=1 prints the result line; any other value appends it to the
+// file it names (unset: nothing, the output stays the reference's).
+inline void report_json(const RunReport &r) {
+    const char *dst = std::getenv("COSPDNN_JSON");
+    if (!dst || !*dst) return;
+    const std::string line = json_line(r);
+    if (std::string(dst) == "1") {
+        std::cout << line << std::endl;
+        return;
+    }
+    std::FILE *f = std::fopen(dst, "a");
+    if (!f) die(std::string("cannot write ") + dst);
+    std::fprintf(f, "%s\n", line.c_str());
+    std::fclose(f);
+}
+
 inline int env_precision() {
     const char *p = std::getenv("COSPDNN_PRECISION");
     const std::string s = p ? p : "fp16";

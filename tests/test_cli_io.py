@@ -59,6 +59,23 @@ int main(int argc, char **argv) {
         triples(argv[2], (size_t)atol(argv[3]));
         return 0;
     }
+    if (mode == "json") {  // json MS ROW... : a result line for a fixed 3-layer network
+        RunReport r;
+        r.program = "cospdnn";
+        r.neuron = 1024;
+        r.batch = 60000;
+        r.layers = 3;
+        r.precision = COSPDNN_PREC_BF16;
+        r.kernel = COSPDNN_KERNEL_TCGEN05;
+        r.gpus = 2;
+        r.weights = 3 * 32768;
+        r.ms = (float)atof(argv[2]);
+        r.alive = {500, 40, 7};
+        r.rechecked = {3, 0, 1};
+        for (int i = 3; i < argc; ++i) r.categories.push_back(atoll(argv[i]));
+        report_json(r);
+        return 0;
+    }
     if (mode == "load" || mode == "parse") {
         const int n = atoi(argv[2]), b = atoi(argv[3]), l = atoi(argv[4]);
         const Network net = mode == "load" ? load_network(n, b, l, argv[5]) : parse_network(n, b, l, argv[5]);
@@ -237,4 +254,37 @@ def test_number_reader_matches_stream_extraction(harness, tmp_path, bad):
         rc, out = _run(harness, ["nums", path, 8192])
         got = dict(line.split(" ", 1) for line in out.strip().splitlines())
         assert got["stream"] == got["reader"], text
+
+
+def test_json_result_line(harness, tmp_path):
+    """COSPDNN_JSON: one JSON line with sizes, device time, edges and
+    edges/s, rows alive and rechecked per layer and the categories' count and
+    hash (the FNV-1a hash of their categories file, as
+    cospdnn_b200.categories computes it); printed for 1, appended to a named
+    file, absent when unset."""
+    import json
+    from cospdnn_b200 import categories as cat
+    rows = [9, 0, 2, 4096]
+    rc, out = _run(harness, ["json", "1.5"] + rows, {"COSPDNN_JSON": "1"})
+    assert rc == 0
+    j = json.loads(out.strip())
+    assert j["program"] == "cospdnn" and "network" not in j
+    assert (j["neuron"], j["batch"], j["layers"], j["gpus"]) == (1024, 60000, 3, 2)
+    assert j["precision"] == "bf16" and j["kernel"] == "tcgen05" and j["weights"] == 98304
+    assert j["ms"] == 1.5 and j["edges"] == 60000 * 98304
+    assert abs(j["edges_per_s"] - 60000 * 98304 / 1.5e-3) / j["edges_per_s"] < 1e-5
+    assert j["alive"] == [500, 40, 7] and j["fp64_rechecked"] == [3, 0, 1]
+    assert j["categories"] == 4 and j["category_hash"] == "fnv1a64:" + cat.digest(rows)
+    f = tmp_path / "cats.tsv"
+    cat.write(f, rows)
+    assert cat.main(["--hash", str(f)]) == 0
+    log = tmp_path / "r.jsonl"
+    for _ in range(2):
+        rc, out = _run(harness, ["json", "2"] + rows, {"COSPDNN_JSON": str(log)})
+        assert rc == 0 and out == ""
+    lines = log.read_text().splitlines()
+    assert len(lines) == 2 and all(json.loads(x)["ms"] == 2 for x in lines)
+    rc, out = _run(harness, ["json", "2"], {"COSPDNN_JSON": ""})
+    assert rc == 0 and out == ""
+    assert cat.digest([]) == "cbf29ce484222325"  # FNV-1a offset basis: no rows
 
