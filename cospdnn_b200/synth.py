@@ -104,6 +104,31 @@ def input_rows(rows, neuron, seed, net=0, dlo=0.08, dhi=0.25, row0=0, fmt=0, dev
     return out
 
 
+def _mix64(z):
+    """SplitMix64's output function on a uint64 array (wrapping arithmetic)."""
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def input_rows_host(rows, neuron, seed, net=0, dlo=0.08, dhi=0.25, row0=0, chunk=256):
+    """The rows input_rows generates on the GPU, computed on the host with
+    numpy (the same bytes, [rows][neuron] uint8), for machines without a GPU:
+    draw 1 of row r's stream gives its density d = dlo + (dhi - dlo) * u,
+    draw j + 2 gives element j = (u < d), u = (draw >> 11) * 2^-53."""
+    out = np.empty((rows, neuron), np.uint8)
+    g = np.uint64(GAMMA)
+    draws = (np.arange(neuron, dtype=np.uint64) + np.uint64(2)) * g
+    scale = 1.0 / 9007199254740992.0
+    for r0 in range(0, rows, chunk):
+        r1 = min(rows, r0 + chunk)
+        s0 = np.array([stream_seed(seed, 2, net, row0 + r) for r in range(r0, r1)], np.uint64)
+        d = dlo + (dhi - dlo) * ((_mix64(s0 + g) >> np.uint64(11)).astype(np.float64) * scale)
+        u = (_mix64(s0[:, None] + draws[None, :]) >> np.uint64(11)).astype(np.float64) * scale
+        out[r0:r1] = u < d[:, None]
+    return out
+
+
 # ---------------------------------------------------------- reference files
 def write_reference_dataset(dirname, neuron, layers, y0, csc_layers, fuse=None):
     """Writes dir/sparse-images-N.tsv, dir/neuronN/N-l{l+1}.tsv and
@@ -124,3 +149,34 @@ def write_reference_dataset(dirname, neuron, layers, y0, csc_layers, fuse=None):
         for l in range(layers):
             row = np.arange(neuron) if fuse is None else fuse[l]
             f.write("\t".join(str(int(x)) for x in row) + "\n")
+
+
+def main(argv=None):
+    """python -m cospdnn_b200.synth OUT_DIR neuron layers batch [--seed S]
+    [--kind xor|r1] [--dlo D] [--dhi D]: a seeded synthetic network and its
+    input rows in the reference's dataset format (identity fuse), generated on
+    the host, for both command lines (ours and the reference's)."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m cospdnn_b200.synth")
+    ap.add_argument("out_dir")
+    ap.add_argument("neuron", type=int)
+    ap.add_argument("layers", type=int)
+    ap.add_argument("batch", type=int)
+    ap.add_argument("--seed", type=int, default=20240611)
+    ap.add_argument("--kind", choices=["xor", "r1"], default="xor")
+    ap.add_argument("--dlo", type=float, default=0.08)
+    ap.add_argument("--dhi", type=float, default=0.25)
+    a = ap.parse_args(argv)
+    if a.neuron <= 0 or a.layers <= 0 or a.batch <= 0 or (a.kind == "r1" and a.neuron % 16):
+        ap.error("neuron, layers and batch must be positive (neuron a multiple of 16 for r1)")
+    y0 = input_rows_host(a.batch, a.neuron, a.seed, dlo=a.dlo, dhi=a.dhi)
+    write_reference_dataset(a.out_dir, a.neuron, a.layers, y0, network(a.neuron, a.layers, a.seed, kind=a.kind))
+    print(f"wrote {a.out_dir}: {a.neuron} neurons x {a.layers} layers ({a.kind}), {a.batch} rows, "
+          f"{int(y0.sum())} input non-zeros")
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())
+
