@@ -143,7 +143,7 @@ def write_reference_dataset(dirname, neuron, layers, y0, csc_layers, fuse=None):
         col = np.repeat(np.arange(neuron), np.diff(cp))
         with open(os.path.join(dirname, f"neuron{neuron}", f"{neuron}-l{l + 1}.tsv"), "w") as f:
             for a, b, v in zip((ri + 1).tolist(), (col + 1).tolist(), vv.tolist()):
-                f.write(f"{a}\t{b}\t{v:.6g}\n")
+                f.write(f"{a}\t{b}\t{v:.9g}\n")  # 9 digits: every float32 reads back exactly
     with open(os.path.join(dirname, "fuse_matrix", f"neuron{neuron}",
                            f"{neuron}_{layers}_fuse.tsv"), "w") as f:
         for l in range(layers):

@@ -288,3 +288,24 @@ def test_json_result_line(harness, tmp_path):
     assert rc == 0 and out == ""
     assert cat.digest([]) == "cbf29ce484222325"  # FNV-1a offset basis: no rows
 
+
+def test_dataset_writer_keeps_float32_weights(harness, tmp_path):
+    """Weights written by synth.write_reference_dataset read back bit for bit
+    through the command lines' reader (random float32 values need 9 digits)."""
+    from cospdnn_b200 import synth
+    from netgen import random_layer
+    n, L, rows = 128, 2, 8
+    layers = []
+    rng = np.random.default_rng(4)
+    for l in range(L):
+        cp, ri, vv = random_layer(n, 40, l)
+        layers.append((cp, ri, rng.standard_normal(len(vv)).astype(np.float32)))
+    y0 = (rng.random((rows, n)) < 0.3).astype(np.uint8)
+    synth.write_reference_dataset(str(tmp_path), n, L, y0, layers)
+    for l, (cp, ri, vv) in enumerate(layers):
+        t = np.loadtxt(tmp_path / f"neuron{n}" / f"{n}-l{l + 1}.tsv", ndmin=2, dtype=str)
+        back = np.array([np.float32(x) for x in t[:, 2]])
+        np.testing.assert_array_equal(back.view(np.uint32), vv.view(np.uint32))
+    rc, out = _run(harness, ["parse", n, rows, L, tmp_path])
+    assert rc == 0 and f"layers {L}" in out
+
