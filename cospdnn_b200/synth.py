@@ -135,10 +135,12 @@ def write_reference_dataset(dirname, neuron, layers, y0, csc_layers, fuse=None):
     dir/fuse_matrix/neuronN/N_L_fuse.tsv in the reference's formats."""
     os.makedirs(os.path.join(dirname, f"neuron{neuron}"), exist_ok=True)
     os.makedirs(os.path.join(dirname, "fuse_matrix", f"neuron{neuron}"), exist_ok=True)
-    r, c = np.nonzero(np.asarray(y0))
+    y0 = np.asarray(y0)
+    r, c = np.nonzero(y0)
+    vals = y0[r, c].astype(np.float32).tolist()
     with open(os.path.join(dirname, f"sparse-images-{neuron}.tsv"), "w") as f:
-        for a, b in zip((r + 1).tolist(), (c + 1).tolist()):
-            f.write(f"{a}\t{b}\t1\n")
+        for a, b, v in zip((r + 1).tolist(), (c + 1).tolist(), vals):
+            f.write(f"{a}\t{b}\t{v:.9g}\n")  # "1" for binary images
     for l, (cp, ri, vv) in enumerate(csc_layers):
         col = np.repeat(np.arange(neuron), np.diff(cp))
         with open(os.path.join(dirname, f"neuron{neuron}", f"{neuron}-l{l + 1}.tsv"), "w") as f:

@@ -307,5 +307,15 @@ def test_dataset_writer_keeps_float32_weights(harness, tmp_path):
         back = np.array([np.float32(x) for x in t[:, 2]])
         np.testing.assert_array_equal(back.view(np.uint32), vv.view(np.uint32))
     rc, out = _run(harness, ["parse", n, rows, L, tmp_path])
-    assert rc == 0 and f"layers {L}" in out
+    assert rc == 0 and f"layers {L}" in out and "integral 1" in out
+    assert (tmp_path / f"sparse-images-{n}.tsv").read_text().split("\n")[0].endswith("\t1")
+    # non-binary rows keep their values
+    y1 = np.where(y0 > 0, rng.random((rows, n)).astype(np.float32) * 3, 0).astype(np.float32)
+    synth.write_reference_dataset(str(tmp_path / "v"), n, L, y1, layers)
+    t = np.loadtxt(tmp_path / "v" / f"sparse-images-{n}.tsv", ndmin=2, dtype=str)
+    back = np.zeros((rows, n), np.float32)
+    back[t[:, 0].astype(int) - 1, t[:, 1].astype(int) - 1] = [np.float32(x) for x in t[:, 2]]
+    np.testing.assert_array_equal(back, y1)
+    rc, out = _run(harness, ["parse", n, rows, L, tmp_path / "v"])
+    assert rc == 0 and "integral 0" in out
 
