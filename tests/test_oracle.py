@@ -120,6 +120,52 @@ def test_ref_layer_transposes_asymmetric_blocks(oracle):
     assert np.count_nonzero(t) == 0 and np.all(t2[3] == 2.0)
 
 
+@pytest.mark.parametrize("tau", [1e-5, 0.0])
+def test_fp64_recurrence_clamp_signs_and_real_inputs(oracle, tau):
+    """The same pin where the plain loop reaches every branch: unstructured
+    weights of both signs up to 4 (outputs above the clamp at 32 and below
+    0), non-binary inputs, threshold 1e-5 or 0; per-layer maxima, the layer a
+    row dies at and the final activations of surviving rows all equal."""
+    n, L, rows, bias = 48, 5, 30, -6.0  # rows die at layers 1 and 2, 18 survive
+    rng = np.random.default_rng(11)
+    layers = []
+    for l in range(L):
+        cp = np.zeros(n + 1, np.int32)
+        ri, vv = [], []
+        for j in range(n):
+            k = int(rng.integers(0, 12))
+            ri += sorted(rng.choice(n, k, replace=False).tolist())
+            vv += (rng.uniform(-4, 4, k) * rng.choice([1, 1, 0.01], k)).astype(np.float32).tolist()
+            cp[j + 1] = cp[j] + k
+        layers.append((cp, np.array(ri, np.int32), np.array(vv, np.float32)))
+    y0 = (rng.random((rows, n)) < 0.5) * rng.uniform(0, 3, (rows, n))
+    y0 = y0.astype(np.float32)
+    res = oracle.infer_fp64(layers, y0, np.float32(bias), tau=tau, want_max=True, want_final=True)
+    b = float(np.float32(bias))
+    clamped = False
+    for r in range(rows):
+        y = y0[r].astype(np.float64)
+        death = L
+        for l, (cp, ri, vv) in enumerate(layers):
+            z = np.empty(n)
+            for j in range(n):
+                acc = 0.0
+                for p in range(cp[j], cp[j + 1]):
+                    if y[ri[p]] != 0:
+                        acc = acc + float(vv[p]) * y[ri[p]]
+                z[j] = acc + b
+            clamped |= bool((z > 32).any())
+            y = np.clip(z, 0.0, 32.0)
+            assert res["maxval"][r, l] == y.max()
+            if not y.max() > tau:
+                death = l
+                break
+        assert res["death"][r] == death
+        if death == L:
+            np.testing.assert_array_equal(res["final"][r], y)
+    assert clamped and 0 < int((res["death"] == L).sum()) < rows
+
+
 def test_cpu_csr_baseline_agrees_with_fp64(oracle):
     n, L, rows = 256, 12, 300
     csc = [oracle.masks_to_csc(oracle.xor_masks(9, 0, l, n), n) for l in range(L)]
