@@ -86,6 +86,8 @@ class NumReader {
     NumReader(const NumReader &) = delete;
     NumReader &operator=(const NumReader &) = delete;
     bool ok() const { return f_ != nullptr; }
+    // a read failed (a directory, an I/O error): the numbers stopped there
+    bool failed() const { return err_; }
     bool next(long &x) {
         if (!token()) return false;
         char *e = nullptr;
@@ -129,6 +131,7 @@ class NumReader {
             if (keep) std::memmove(buf_.data(), p_, keep);
             const size_t got = f_ ? std::fread(buf_.data() + keep, 1, block_ - keep, f_) : 0;
             eof_ = got < block_ - keep;
+            if (eof_ && f_ && std::ferror(f_)) err_ = true;
             p_ = buf_.data();
             end_ = p_ + keep + got;
             *end_ = '\0';  // strtol/strtof stop here
@@ -138,7 +141,7 @@ class NumReader {
     size_t block_;
     std::vector<char> buf_;
     char *p_ = nullptr, *end_ = nullptr;
-    bool eof_ = false;
+    bool eof_ = false, err_ = false;
 };
 
 // Dense rows [batch][neuron]; `integral` stays true while every value is an
@@ -166,6 +169,7 @@ inline std::string read_input(int neuron, int batch, const std::string &dir, Inp
         if (!(val >= 0.0f && val <= 255.0f && (float)(int)val == val)) in.integral = false;
         ++in.read;
     }
+    if (f.failed()) return "FILE:" + name + " cannot be read.";
     return "";
 }
 
@@ -179,7 +183,7 @@ inline std::string read_fuse(int neuron, int layers, const std::string &dir, std
     for (int l = 0; l < layers; ++l)
         for (int j = 0; j < neuron; ++j) {
             float t;
-            if (!f.next(t)) return " read error";
+            if (!f.next(t)) return f.failed() ? "FILE:" + name + " cannot be read." : " read error";
             fuse[l][j] = (int32_t)t;
             if (fuse[l][j] < 0 || fuse[l][j] >= neuron) return "fuse entry out of range in " + name;
         }
@@ -206,6 +210,7 @@ inline std::string read_layer(int neuron, int l, const std::vector<int32_t> &fus
         if (u < 1 || u > neuron || v < 1 || v > neuron) return "weight index out of range in " + name;
         cols[v - 1].push_back({fuse[u - 1], val});
     }
+    if (f.failed()) return "File:" + name + " cannot be read.";
     c = Csc();
     c.colptr.assign(neuron + 1, 0);
     for (int j = 0; j < neuron; ++j) {

@@ -64,6 +64,8 @@ def test_cli_writes_cache_before_it_needs_a_device(tmp_path):
     ("fuse_entry", "fuse entry out of range in"),
     ("fuse_short", "read error"),
     ("image_neuron", "input neuron index out of range in"),
+    ("layer_is_dir", "64-l2.tsv cannot be read."),
+    ("images_is_dir", "sparse-images-64.tsv cannot be read."),
 ])
 def test_cli_bad_dataset_files(tmp_path, fault, message):
     """Damaged dataset files end the run with the reference's kind of message
@@ -84,6 +86,12 @@ def test_cli_bad_dataset_files(tmp_path, fault, message):
         fuse.write_text("64 " + fuse.read_text())
     elif fault == "fuse_short":
         fuse.write_text(fuse.read_text().split("\n")[0] + "\n")
+    elif fault == "layer_is_dir":
+        (d / "neuron64" / "64-l2.tsv").unlink()
+        (d / "neuron64" / "64-l2.tsv").mkdir()
+    elif fault == "images_is_dir":
+        (d / "sparse-images-64.tsv").unlink()
+        (d / "sparse-images-64.tsv").mkdir()
     else:
         with open(d / "sparse-images-64.tsv", "a") as f:
             f.write("1\t65\t1\n")
