@@ -416,6 +416,8 @@ inline bool write_categories(const std::string &path, const std::vector<int64_t>
 // 1-based ids of a categories file; false when it cannot be read or holds
 // anything but positive integers
 inline bool read_categories(const std::string &path, std::vector<int64_t> &ids) {
+    struct stat st;
+    if (stat(path.c_str(), &st) != 0 || !S_ISREG(st.st_mode)) return false;  // a directory reads as empty
     std::ifstream f(path);
     if (!f) return false;
     ids.clear();

@@ -188,6 +188,8 @@ def test_categories_cli_helpers(harness, tmp_path):
     truth.write_text("1\nx\n")
     rc, text = _run(harness, ["cats", 0], env)
     assert rc != 0 and "cannot read truth file" in text
+    rc, text = _run(harness, ["cats", 0], dict(env, COSPDNN_TRUTH=str(tmp_path)))  # a directory
+    assert rc != 0 and "cannot read truth file" in text
 
 
 def test_categories_module(tmp_path):
