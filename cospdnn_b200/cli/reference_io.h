@@ -581,16 +581,18 @@ inline void report_json(const RunReport &r) {
 
 inline int env_precision() {
     const char *p = std::getenv("COSPDNN_PRECISION");
-    const std::string s = p ? p : "fp16";
+    const std::string s = p && *p ? p : "fp16";
     if (s == "fp32") return COSPDNN_PREC_FP32;
     if (s == "bf16") return COSPDNN_PREC_BF16;
+    if (s != "fp16") die("COSPDNN_PRECISION must be fp32, fp16 or bf16, not " + s);
     return COSPDNN_PREC_FP16;
 }
 inline int env_kernel() {
     const char *p = std::getenv("COSPDNN_KERNEL");
-    const std::string s = p ? p : "auto";
+    const std::string s = p && *p ? p : "auto";
     if (s == "cuda-core") return COSPDNN_KERNEL_CUDA_CORE;
     if (s == "tcgen05") return COSPDNN_KERNEL_TCGEN05;
+    if (s != "auto") die("COSPDNN_KERNEL must be auto, cuda-core or tcgen05, not " + s);
     return COSPDNN_KERNEL_AUTO;
 }
 

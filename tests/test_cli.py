@@ -101,6 +101,17 @@ def test_cli_bad_dataset_files(tmp_path, fault, message):
     assert message in out.stdout, out.stdout
 
 
+@pytest.mark.parametrize("var,value", [("COSPDNN_PRECISION", "fp8"), ("COSPDNN_KERNEL", "wgmma")])
+def test_cli_rejects_unknown_settings(tmp_path, var, value):
+    """An unknown precision or kernel name is an error, not the default."""
+    from cospdnn_b200 import synth
+    csc, y0, _ = make_net(64, 2, 10, seed=4, dlo=0.2, dhi=0.4)
+    synth.write_reference_dataset(str(tmp_path), 64, 2, y0, csc)
+    out = subprocess.run([_exe("cospdnn"), "64", "10", "2", "1", "0", str(tmp_path)], capture_output=True,
+                         text=True, timeout=120, env=dict(os.environ, CUDA_VISIBLE_DEVICES="", **{var: value}))
+    assert out.returncode != 0 and f"{var} must be" in out.stdout
+
+
 def _dataset(tmp, n, L, rows, seed, net):
     """Writes a net in the reference's formats with a random fuse per layer and
     returns the oracle's view (weights folded through the fuse)."""
