@@ -228,7 +228,11 @@ def main(argv=None):
     layers = int(argv[3])
     if workers is None:  # one process per layer, up to the host's cores
         workers = min(layers, os.cpu_count() or 1)
-    stats = reorder_dataset(argv[0], argv[1], int(argv[2]), layers, workers=workers)
+    try:
+        stats = reorder_dataset(argv[0], argv[1], int(argv[2]), layers, workers=workers)
+    except (OSError, ValueError) as e:  # missing or damaged dataset files
+        print(f"reorder: {e}")
+        return 1
     b0 = sum(s[0] for s in stats)
     b1 = sum(s[1] for s in stats)
     print(f"greedy 16x16 blocks: {b0} -> {b1} over {len(stats)} layers")

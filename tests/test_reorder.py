@@ -134,3 +134,17 @@ def test_block_count_matches_reference_builder_fixtures(name):
     g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
     n = int(max(g["row"].max(), g["col"].max())) + 1
     assert ro.greedy_blocks(g["row"], g["col"], n, int(g["bs"])) == len(g["row_index"])
+
+
+def test_main_reports_missing_or_damaged_files(tmp_path, capsys):
+    from cospdnn_b200 import synth
+    n = 64
+    assert ro.main([str(tmp_path / "none"), str(tmp_path / "out"), str(n), "2", "--workers", "1"]) == 1
+    assert "reorder: " in capsys.readouterr().out
+    layers = [random_layer(n, 3, l) for l in range(2)]
+    synth.write_reference_dataset(str(tmp_path / "src"), n, 2, np.ones((2, n), np.uint8), layers)
+    with open(tmp_path / "src" / f"neuron{n}" / f"{n}-l2.tsv", "a") as f:
+        f.write("65\t1\t0.5\n")
+    assert ro.main([str(tmp_path / "src"), str(tmp_path / "out"), str(n), "2", "--workers", "1"]) == 1
+    assert "index out of range" in capsys.readouterr().out
+
