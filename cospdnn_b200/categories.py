@@ -60,13 +60,17 @@ def check(rows0, truth_path):
 
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
-    if len(argv) == 2 and argv[0] == "--hash":
-        print(f"fnv1a64:{digest(read(argv[1]))}")
-        return 0
     if len(argv) != 2:
         print("usage: python -m cospdnn_b200.categories OURS TRUTH | --hash FILE")
         return 1
-    r = check(read(argv[0]), argv[1])
+    try:
+        if argv[0] == "--hash":
+            print(f"fnv1a64:{digest(read(argv[1]))}")
+            return 0
+        r = check(read(argv[0]), argv[1])
+    except (OSError, ValueError) as e:  # a missing or malformed file (status 2 is a mismatch)
+        print(f"categories: {e}")
+        return 1
     print(f"categories check: {'PASS' if r['ok'] else 'FAIL'} (ours {r['ours']}, truth {r['truth']}, "
           f"missing {r['missing'].size}, extra {r['extra'].size})")
     return 0 if r["ok"] else 2

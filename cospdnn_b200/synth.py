@@ -172,7 +172,11 @@ def main(argv=None):
     if a.neuron <= 0 or a.layers <= 0 or a.batch <= 0 or (a.kind == "r1" and a.neuron % 16):
         ap.error("neuron, layers and batch must be positive (neuron a multiple of 16 for r1)")
     y0 = input_rows_host(a.batch, a.neuron, a.seed, dlo=a.dlo, dhi=a.dhi)
-    write_reference_dataset(a.out_dir, a.neuron, a.layers, y0, network(a.neuron, a.layers, a.seed, kind=a.kind))
+    try:
+        write_reference_dataset(a.out_dir, a.neuron, a.layers, y0, network(a.neuron, a.layers, a.seed, kind=a.kind))
+    except OSError as e:
+        print(f"synth: {e}")
+        return 1
     print(f"wrote {a.out_dir}: {a.neuron} neurons x {a.layers} layers ({a.kind}), {a.batch} rows, "
           f"{int(y0.sum())} input non-zeros")
     return 0

@@ -211,6 +211,9 @@ def test_categories_module(tmp_path):
     bad.write_text("0\n")
     with pytest.raises(ValueError):
         cat.read(bad)
+    assert cat.main([str(bad), str(p)]) == 1                  # malformed: an error, not a mismatch
+    assert cat.main([str(tmp_path / "none.tsv"), str(p)]) == 1
+    assert cat.main(["--hash", str(tmp_path / "none.tsv")]) == 1
 
 
 def _fmt_triples(rng, n):

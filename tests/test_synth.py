@@ -68,3 +68,6 @@ def test_dataset_command(oracle, tmp_path, capsys):
     np.testing.assert_array_equal(fuse, np.tile(np.arange(64), (3, 1)))
     with pytest.raises(SystemExit):
         synth.main([str(out), "60", "1", "1", "--kind", "r1"])
+    blocker = tmp_path / "file"
+    blocker.write_text("")
+    assert synth.main([str(blocker / "d"), "64", "1", "2"]) == 1  # cannot create the directory
