@@ -602,6 +602,7 @@ extern "C" int cospdnn_engine_add_net(cospdnn_engine *e, const cospdnn_net_desc 
     CSP_CHECK(!(d->kernel == COSPDNN_KERNEL_TCGEN05 && d->precision == COSPDNN_PREC_FP32),
               COSPDNN_ERR_UNSUPPORTED, "add_net: tcgen05 kernel needs FP16 or BF16");
     CSP_CHECK(d->threshold >= 0.0f && d->threshold < 32.0f, COSPDNN_ERR_INVALID, "add_net: threshold outside [0,32)");
+    CSP_CHECK(std::isfinite(d->bias), COSPDNN_ERR_INVALID, "add_net: non-finite bias");
     Net net;
     net.d = *d;
     net.layers.resize(d->layers);
