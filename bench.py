@@ -73,9 +73,10 @@ def edges(nets):
     return float(sum(b * l * 32 * n for n, l, b in nets))
 
 
-# DRAM bytes (read + write) per input row of one layer launch of the
-# dominant kernel, from one ncu capture of a smaller case of the same
-# workload (profiles/k_layer_*.md): traffic grows with the rows processed.
+# DRAM bytes (read + write) per input row of one launch of the config's
+# dominant layer kernel, from one ncu capture of a smaller case of the same
+# kernel on the same weights (profiles/k_layer_*.md): traffic grows with the
+# rows a launch processes.
 DRAM_BYTES_PER_ROW = {
     "c2": (135.131136e6 + 88.350208e6) / 16384,  # k_layer_cc_4096n_16384rows_fp16.md
     "c1": (135.193088e6 + 88.413696e6) / 32768,  # k_layer_cc_1024n_32768rows_fp32.md
@@ -83,13 +84,52 @@ DRAM_BYTES_PER_ROW = {
     "r1": (134.869248e6 + 83.793152e6) / 16384,  # k_layer_tc_4096n_16384rows_r1_fp16.md
 }
 
-
 def measured_peaks():
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json,
+    burst figure: the layer kernels are timed alone), else the fallback."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["hbm_gbs"]), "measured"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     return 6650.0, "fallback"
+
+
+TNAME = {"fp32": "float", "fp16": "__half", "bf16": "__nv_bfloat16"}
+# rows per network that the FP64 parity check replays (the whole batch where
+# the oracle finishes in seconds, else the first rows of it)
+PARITY_ROWS = {1024: 60000, 4096: 60000, 16384: 16384, 65536: 2048}
+DY_ROWS = 2048  # rows per checked layer compared value by value
+
+
+def layer_kernel_name(info, n, prec):
+    """Name of the kernel that computes layers >= 1 of a net (engine's choice)."""
+    import cospdnn_b200 as cs
+    es = 4 if prec == "fp32" else 2
+    if info["kernel"] == cs.KERNEL_TCGEN05:
+        return f"k_layer_tc<{TNAME[prec]}>"
+    tr = info["row_tile"]
+    if tr == 0:
+        return f"k_layer_plain<{TNAME[prec]}>"
+    nt = 256 if n * tr * es <= 96 * 1024 else 512
+    lb = 16 if tr * es >= 16 else 8
+    return f"k_layer_cc<{TNAME[prec]}, {nt}, {lb}>"
+
+
+def layer0_kernel_name(info, prec):
+    import cospdnn_b200 as cs
+    if not info["layer0_counted"]:
+        return None
+    return f"k_layer0_bits16<{TNAME[prec]}>" if info["kernel"] == cs.KERNEL_TCGEN05 else f"k_layer0_bits<{TNAME[prec]}>"
+
+
+def weight_bytes(info, n, prec):
+    """Bytes of W_l the layer kernel reads (32 entries per output)."""
+    import cospdnn_b200 as cs
+    if info["kernel"] == cs.KERNEL_TCGEN05:
+        return 32.0 * (n // 16) * 512  # about one 16x16 operand per entry group of a block column
+    if info["row_tile"] and prec != "fp32":
+        return 32.0 * n * 4  # (input column << 16 | weight) per entry
+    return 32.0 * n * 8      # int32 index + float weight per entry
 
 
 class Clocks:
@@ -165,14 +205,13 @@ def sample_rows(run, total, budget_s):
         rows = int(min(total, rows * max(2.0, min(8.0, 0.8 * budget_s / max(dt, 1e-3)))))
 
 
-def cpu_baseline(nets, dens, y0_host_fn, budget_s=12.0, threads=None, kind="xor"):
+def cpu_baseline(nets, dens, y0_host_fn, weights, budget_s=12.0, threads=None):
     """Multithreaded FP32 CSR recurrence (oracle/ port) on a bounded row sample."""
-    from cospdnn_b200 import synth
     from oracle import pyoracle as po
     threads = threads or os.cpu_count()
     total_edges, total_t, desc = 0.0, 0.0, []
     for i, (n, L, b) in enumerate(nets):
-        csr = [po.coo_to_csr(*po.csc_to_coo(*c), n) for c in synth.network(n, L, SEED, net=i, kind=kind)]
+        csr = [po.coo_to_csr(*po.csc_to_coo(*c), n) for c in weights[i]]
         bias = np.float32({1024: -0.3, 4096: -0.35, 16384: -0.4, 65536: -0.45}[n])
         rows = sample_rows(lambda r: po.infer_fp32_csr(csr, y0_host_fn(i, r), bias, threads=threads),
                            b, budget_s / len(nets))
@@ -185,6 +224,120 @@ def cpu_baseline(nets, dens, y0_host_fn, budget_s=12.0, threads=None, kind="xor"
         desc.append(f"{rows} of {b} rows of net {i} ({n}x{L})")
     return {"value": total_edges / total_t, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": "; ".join(desc) + f"; {total_t:.1f} s on {threads} threads, FP32 CSR, early exit"}
+
+
+def parity_check(cs, nets, prec, kernel, dens, weights, local, stream, inputs):
+    """The FP64 oracle as checker of the benched configuration: an engine of
+    the same networks (weights, precision, kernel choice) on the first rows of
+    each batch (all of them where the oracle finishes in seconds), whose
+    per-layer survivor counts and categories are compared with the oracle's,
+    and whose outputs at up to four layers with survivors (first, last and
+    two between; up to DY_ROWS rows each) are compared value by value with
+    the oracle's FP64 replay of the same rows (max |dY|, and whether every
+    row's |dY| lies within the error bound the engine carries for it)."""
+    from oracle import pyoracle as po
+    threads = os.cpu_count()
+    rows = [min(b, PARITY_ROWS.get(n, 2048)) for n, _, b in nets]
+    eng = cs.Engine(local)
+    ids = []
+    for i, (n, L, b) in enumerate(nets):
+        nid = eng.add_net(n, L, rows[i], cs.BIAS[n], cs.THRESHOLD, PREC[prec], kernel)
+        for l, (cp, ri, vv) in enumerate(weights[i]):
+            eng.set_layer_csc(nid, l, cp, ri, vv)
+        ids.append(nid)
+    eng.build()
+    for nid, y, r in zip(ids, inputs, rows):
+        eng.set_input(nid, y[:r], stream=stream)
+    eng.run(stream)
+    alive_eq, cats_eq, dy, dy_rows, dy_layers, within = True, True, 0.0, 0, [], True
+    for i, (nid, (n, L, b)) in enumerate(zip(ids, nets)):
+        res = eng.result(nid, stream)
+        y0 = inputs[i][:rows[i]].cpu().numpy()
+        bias = np.float32(cs.BIAS[n])
+        ref = po.infer_fp64(weights[i], y0, bias, threads=threads)
+        alive_ref = po.survivors_per_layer(ref["death"], L)
+        alive_eq &= bool(np.array_equal(res["alive"], alive_ref))
+        cats_eq &= bool(np.array_equal(res["categories"], np.nonzero(ref["death"] == L)[0]))
+        live = [l for l in range(L) if alive_ref[l] > 0]
+        if live:
+            pick = sorted({live[0], live[len(live) // 3], live[(2 * len(live)) // 3], live[-1]})
+            for l in pick:
+                vals, rid, bnd = eng.layer_values(nid, l, max_rows=DY_ROWS, stream=stream, bounds=True)
+                if len(rid) == 0:
+                    continue
+                want = po.replay_fp64(weights[i], y0, bias, rid.astype(np.int64), l)
+                d = np.abs(vals.astype(np.float64) - want).max(axis=1)
+                dy = max(dy, float(d.max()))
+                within &= bool(np.all(d <= bnd.astype(np.float64)))
+                dy_rows += len(rid)
+                dy_layers.append((i, l))
+    eng.close()
+    return {"rows_checked": [int(r) for r in rows], "alive_equal": alive_eq, "categories_equal": cats_eq,
+            "max_abs_dy": dy, "dy_within_proven_bound": within,
+            "dy_rows_checked": int(dy_rows), "dy_layers": [f"net {i} layer {l}" for i, l in dy_layers],
+            "oracle": "FP64 recurrence, fixed summation order (oracle/oracle.c), "
+                      f"{threads} threads; values compared after each listed layer for up to "
+                      f"{DY_ROWS} of its kept rows"}
+
+
+def reference_cuda_build(nets, kind, dens):
+    """The reference's own host loop and kernels (test_graph_challenge_tc,
+    compiled from its sources for sm_100a into oracle/_ref) on the same
+    weights and inputs, one run; its printed "Kernel Exec Time" and the wall
+    time of the call.  Single networks up to 4096 neurons (its host code
+    takes minutes beyond that).  On XOR-mask weights its kernel reads two
+    16x16 blocks per block column (src/kernels/kernel.cu:257), so its product
+    is truncated: timing only."""
+    import ctypes as C
+    so = os.path.join(ROOT, "oracle", "_ref", "libref_cospdnn.so")
+    if len(nets) != 1 or nets[0][0] > 4096:
+        return {"unavailable": "measured for single networks of at most 4096 neurons"}
+    if not os.path.exists(so):
+        return {"unavailable": "oracle/_ref/libref_cospdnn.so not built (make -C oracle ref REF=...)"}
+    from cospdnn_b200 import synth
+    from oracle import pyoracle as po
+    n, L, b = nets[0]
+    csc = synth.network(n, L, SEED, net=0, kind=kind)
+    vals, rws, ptrs = [], [], []
+    for cp, ri, vv in csc:
+        row, col, val = po.csc_to_coo(cp, ri, vv)
+        bcp, bri, _, bvals = po.bcsc_greedy(row, col, val, 16)
+        # its kernel reads the first two blocks of every column, 16 fuse rows each
+        if not (np.all(np.diff(bcp) >= 2) and bri[bcp[:-1]].max() <= n - 16 and bri[bcp[:-1] + 1].max() <= n - 16):
+            return {"unavailable": "weights outside what the reference kernel reads in bounds"}
+        vals.append(np.ascontiguousarray(bvals, np.float32))
+        rws.append(np.ascontiguousarray(bri, np.int32))
+        ptrs.append(np.ascontiguousarray(bcp, np.int32))
+    fp, ip = C.POINTER(C.c_float), C.POINTER(C.c_int)
+    V = (fp * L)(*[v.ctypes.data_as(fp) for v in vals])
+    RI = (ip * L)(*[r.ctypes.data_as(ip) for r in rws])
+    P = (ip * L)(*[q.ctypes.data_as(ip) for q in ptrs])
+    nv = np.array([len(v) for v in vals], np.int64)
+    nr = np.array([len(r) for r in rws], np.int64)
+    npp = np.array([len(q) for q in ptrs], np.int64)
+    feats = np.full(64, -1, np.int32)
+    kms, wms, last = C.c_double(), C.c_double(), C.c_int()
+    tail = C.create_string_buffer(4096)
+    ref = C.CDLL(so)
+    ref.ref_run_network.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_void_p]
+    y = np.ascontiguousarray(po.input_binary(SEED, 0, b, n, dens[0], dens[1]), np.uint8)
+    bias = {1024: -0.3, 4096: -0.35, 16384: -0.4, 65536: -0.45}[n]
+    rc = ref.ref_run_network(y.ctypes.data, b, n, L, C.addressof(V), nv.ctypes.data, C.addressof(RI),
+                             nr.ctypes.data, C.addressof(P), npp.ctypes.data, float(bias), C.addressof(kms),
+                             C.addressof(wms), C.addressof(last), feats.ctypes.data, 64, tail, 4096, None)
+    if rc != 0:
+        return {"unavailable": f"reference run failed: {tail.value.decode(errors='replace')[-200:]}"}
+    e = float(b) * L * 32 * n
+    return {"kernel_exec_ms": kms.value, "wall_ms": wms.value, "edges_per_s_kernel": e / (kms.value * 1e-3),
+            "edges_per_s_wall": e / (wms.value * 1e-3),
+            "printed_features": [int(x) for x in feats[:8] if x >= 0],
+            "note": ("its Kernel Exec Time covers its SpMM kernels only (src/cospdnn.cu:303-310); wall "
+                     "covers its whole host loop. " +
+                     ("Timing only: XOR-mask weights have 19-32 blocks per block column and its kernel "
+                      "reads two, so its product is truncated." if kind == "xor" else
+                      "R1 weights: two aligned dense blocks per block column, computed in full."))}
 
 
 def run_reference(args, nets, prec, dens):
@@ -221,6 +374,12 @@ def run_reference(args, nets, prec, dens):
     t = sum(times) / len(times)
     value = step_edges / t
     sample = ", ".join(f"{rows} of {nets[i][2]} rows of net {i}" for i, rows, _, _ in samples)
+    ref_build = None
+    if not args.no_reference_build:
+        try:
+            ref_build = reference_cuda_build(nets, weight_kind(args.config), dens)
+        except Exception as ex:  # reported, not fatal: the arm's value is the CPU port
+            ref_build = {"unavailable": f"{type(ex).__name__}: {ex}"}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -233,8 +392,49 @@ def run_reference(args, nets, prec, dens):
                                             f"early exit; the reference has no CPU implementation "
                                             f"of this path"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda_build": ref_build,
     }
     print(json.dumps(line), flush=True)
+
+
+def build_engine(cs, nets, prec, kernel, weights, local, rows=None):
+    eng = cs.Engine(local)
+    ids = []
+    for i, (n, L, b) in enumerate(nets):
+        nid = eng.add_net(n, L, b if rows is None else rows[i], cs.BIAS[n], cs.THRESHOLD, PREC[prec], kernel)
+        for l, (cp, ri, vv) in enumerate(weights[i]):
+            eng.set_layer_csc(nid, l, cp, ri, vv)
+        ids.append(nid)
+    eng.build()
+    return eng, ids
+
+
+def time_device(torch, eng, stream, steps, warmup, flush, clocks=None):
+    """Mean device time of one run over `steps` runs (CUDA events on the
+    launching stream around each run), after `warmup` runs; between timed runs
+    (outside the events) a write of `flush` evicts L2."""
+    for _ in range(warmup):
+        eng.run(stream)
+    stream.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        for e0, e1 in evs:
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0.record(stream)
+            eng.run(stream)
+            e1.record(stream)
+        stream.synchronize()
+    return sum(e0.elapsed_time(e1) for e0, e1 in evs) / steps
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
 
 
 def main():
@@ -246,8 +446,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=[None, "fp32", "fp16", "bf16"])
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 CUDA cores, 2 tcgen05")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU baseline and the FP64 parity check")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the plain-FP32 arm of the same engine")
+    ap.add_argument("--no-reference-build", action="store_true",
+                    help="--impl reference: skip timing the reference's own CUDA build")
     ap.add_argument("--rows", type=int, default=None, help="override the rows per network (profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -273,16 +476,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device(f"cuda:{local}"))
     stream = torch.cuda.Stream()
+    # L2 is 126 MB: a 256 MB write between timed runs evicts it
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     # ---- setup (untimed): weights replicated, each rank its own rows
-    eng = cs.Engine(local)
-    ids, inputs = [], []
-    for i, (n, L, b) in enumerate(nets):
-        nid = eng.add_net(n, L, b, cs.BIAS[n], cs.THRESHOLD, PREC[prec], args.kernel)
-        for l, (cp, ri, vv) in enumerate(synth.network(n, L, SEED, net=i, kind=weight_kind(args.config))):
-            eng.set_layer_csc(nid, l, cp, ri, vv)
-        ids.append(nid)
-    eng.build()
+    kind = weight_kind(args.config)
+    weights = [synth.network(n, L, SEED, net=i, kind=kind) for i, (n, L, b) in enumerate(nets)]
+    eng, ids = build_engine(cs, nets, prec, args.kernel, weights, local)
+    inputs = []
     with torch.cuda.stream(stream):
         for i, (n, L, b) in enumerate(nets):
             inputs.append(synth.input_rows(b, n, SEED, net=i, dlo=dens[0], dhi=dens[1],
@@ -303,68 +504,81 @@ def main():
         from cospdnn_b200 import dist as cd
         return cd.max_over_ranks(x, device=f"cuda:{local}")
 
-    # ---- device-resident timing
-    for _ in range(args.warmup):
-        eng.run(stream)
+    # ---- device-resident timing: one graph launch per step, L2 evicted between steps
     barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        barrier()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            eng.run(stream)
-        ev1.record(stream)
-        ev1.synchronize()
-        barrier()
-    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    clk = Clocks(local)
+    ms = max_over_ranks(time_device(torch, eng, stream, args.steps, args.warmup, flush, clocks=clk))
+    barrier()
     launches_per_run = eng.launch_count(stream)
     results = [eng.result(nid, stream) for nid in ids]
+    infos = [eng.net_info(nid, stream) for nid in ids]
     step_edges = edges(nets)
     value = step_edges * world / (ms * 1e-3)
 
-    # ---- per-layer kernel times (eager pass of the same kernels) -> roofline
-    iters_max = max(L for _, L, _ in nets) + 1
-    import ctypes as C
-    lms = np.zeros(iters_max, np.float32)
-    nit = C.c_int()
-    cs._check(cs.lib().cospdnn_engine_profile_layers(
-        eng._h, cs._stream(stream), iters_max, lms.ctypes.data_as(C.POINTER(C.c_float)),
-        C.byref(nit)))
-    nit = nit.value
+    # ---- roofline of the dominant kernel from the per-iteration layer-kernel
+    # times of an eager pass of the same kernels (CUDA events on `stream`)
+    lms = eng.profile_layers(stream=stream)
+    nit = len(lms)
     es = 4 if prec == "fp32" else 2
-    layer_bytes = np.zeros(nit)
-    for r, (n, L, b) in zip(results, nets):
+    b_l0 = np.zeros(nit)
+    b_ly = np.zeros(nit)
+    rows_ly = np.zeros(nit)
+    for r, info, (n, L, b) in zip(results, infos, nets):
         rows_in = np.concatenate([[b], r["alive"][:-1]])
         for it in range(min(nit, L)):
-            R = rows_in[it]
-            if R > 0:
-                # algorithmic bytes: active input rows read + their outputs written + W
-                layer_bytes[it] += 2.0 * R * n * es + 32.0 * n * 8
-    per_layer = [{"iter": i, "ms": float(lms[i]), "GBps": float(layer_bytes[i] / (lms[i] * 1e-3) / 1e9)
-                  if lms[i] > 0 else 0.0} for i in range(nit)]
+            R = float(rows_in[it])
+            if R <= 0:
+                continue
+            if it == 0 and info["layer0_counted"]:
+                # bit planes read, outputs written, the layer-0 schedule
+                b_l0[it] += R * n / 8 + R * n * es + 32.0 * n * 2 + 4.0 * n
+            else:
+                # active input rows read, their outputs written, W
+                b_ly[it] += 2.0 * R * n * es + weight_bytes(info, n, prec)
+                rows_ly[it] += R
+    # iteration 0 is the counting kernel when every net counted layer 0
+    l0_iter = all(i["layer0_counted"] for i in infos)
+    t_l0 = float(lms[0]) if (nit and l0_iter) else 0.0
+    it_ly = [i for i in range(nit) if not (i == 0 and l0_iter) and b_ly[i] > 0]
+    t_ly = float(sum(lms[i] for i in it_ly))
     peak, peak_kind = measured_peaks()
-    tot_b, tot_t = float(layer_bytes.sum()), float(lms[:nit].sum()) * 1e-3
-    achieved = tot_b / tot_t / 1e9 if tot_t > 0 else 0.0
-    rows_per_launch = 0.0
-    for r, (n, L, b) in zip(results, nets):
-        rows_in = np.concatenate([[b], r["alive"][:-1]])
-        rows_per_launch += float(rows_in[:min(nit, L)].sum()) / max(1, nit)
+    names = sorted({layer_kernel_name(i, n, prec) for i, (n, _, _) in zip(infos, nets)})
+    l0_names = sorted({x for x in (layer0_kernel_name(i, prec) for i in infos) if x})
+    per_layer = []
+    for i in range(min(nit, 8)):
+        bb = b_l0[i] + b_ly[i]
+        per_layer.append({"iter": i, "kernel": (" + ".join(l0_names) if (i == 0 and l0_iter) else " + ".join(names)),
+                          "ms": float(lms[i]), "bytes": bb,
+                          "GBps": float(bb / (lms[i] * 1e-3) / 1e9) if lms[i] > 0 else 0.0})
+    dominant_is_l0 = l0_iter and t_l0 > t_ly
+    if dominant_is_l0:
+        kname, kb, kt, klaunch = " + ".join(l0_names), float(b_l0[0]), t_l0, 1
+    else:
+        kname, kb, kt, klaunch = " + ".join(names), float(sum(b_ly[i] for i in it_ly)), t_ly, max(1, len(it_ly))
+    achieved = kb / (kt * 1e-3) / 1e9 if kt > 0 else 0.0
     traffic = None
-    if args.config in DRAM_BYTES_PER_ROW and args.precision in (None, prec) and args.kernel == 0:
-        traffic = DRAM_BYTES_PER_ROW[args.config] * rows_per_launch
+    if (not dominant_is_l0 and args.config in DRAM_BYTES_PER_ROW and args.precision in (None, prec)
+            and args.kernel == 0 and it_ly):
+        traffic = DRAM_BYTES_PER_ROW[args.config] * float(sum(rows_ly[i] for i in it_ly)) / len(it_ly)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "layer kernels of the net (bit-count layer 0 for binary inputs; row-tile CUDA-core, "
-                          "tcgen05 or row-major gather)",
-                "traffic_note": "DRAM bytes per launch scaled from an ncu capture of a smaller case "
-                                "(per input row) to this workload's average rows per layer launch",
-                "bytes_per_launch": tot_b / max(1, nit),
-                "ms_per_launch": float(lms[:nit].mean()) if nit else 0.0,
-                "per_layer": per_layer[:8]}
+                "kernel": kname, "launches": klaunch, "bytes_per_launch": kb / klaunch,
+                "ms_per_launch": kt / klaunch,
+                "bytes_rule": ("per launch: active input rows x N x elem read + their outputs written + W_l "
+                               "(layer 0 counted from bits: R x N / 8 bytes of bit planes + outputs + schedule)"),
+                "traffic_note": ("DRAM bytes per launch scaled from an ncu capture of a smaller case of the same "
+                                 "kernel (per input row) to this workload's rows per launch; null where no "
+                                 "capture of this kernel and config is committed"),
+                "layer0": ({"kernel": " + ".join(l0_names), "ms": t_l0, "bytes": float(b_l0[0]),
+                            "GBps": float(b_l0[0] / (t_l0 * 1e-3) / 1e9) if t_l0 > 0 else 0.0,
+                            "frac": float(b_l0[0] / (t_l0 * 1e-3) / 1e9 / peak) if t_l0 > 0 else 0.0}
+                           if l0_iter else None),
+                "per_layer": per_layer}
 
     # ---- end to end through the public API: pinned host Y0 -> H2D -> run -> D2H result
     e2e = None
     if not args.no_e2e:
+        import ctypes as C
         # the rows are binary: hand them over as packed bits (1 bit per feature,
         # COSPDNN_INPUT_BITS), the compact form of a Graph Challenge input
         host_in = [torch.from_numpy(np.packbits(y.cpu().numpy(), axis=1, bitorder="little")).pin_memory()
@@ -405,6 +619,7 @@ def main():
                     set_inputs(k + 1)
             stream.synchronize()
 
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e2e_steps(args.warmup)
         barrier()
         t0 = time.perf_counter()
@@ -419,13 +634,36 @@ def main():
         assert cnt == len(results[0]["categories"]), "e2e result differs from device-resident run"
         e2e = {"value": step_edges * world / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-               "input": "binary rows as packed bits (COSPDNN_INPUT_BITS) from pinned host memory; "
-                        "result (count, alive per layer, categories) read back every step; the next "
-                        "step's copy and conversion overlap the current run (double-buffered inputs)"}
+               "input": "binary rows as packed bits (COSPDNN_INPUT_BITS) copied from pinned host memory "
+                        "every step; result (count, alive per layer, categories) read back every step; the "
+                        "next step's copy and conversion overlap the current run (double-buffered inputs)"}
+    eng.close()
+    del eng
 
-    cpu = None
+    # ---- the plain FP32 path of the same engine on the same workload
+    fp32 = None
+    if not args.no_fp32 and prec != "fp32":
+        e32, ids32 = build_engine(cs, nets, "fp32", 0, weights, local)
+        for nid, y in zip(ids32, inputs):
+            e32.set_input(nid, y, stream=stream)
+        k32 = min(args.steps, 10)
+        ms32 = max_over_ranks(time_device(torch, e32, stream, k32, 3, flush))
+        r32 = [e32.result(nid, stream) for nid in ids32]
+        info32 = [e32.net_info(nid, stream) for nid in ids32]
+        same = all(np.array_equal(a["categories"], b["categories"]) and np.array_equal(a["alive"], b["alive"])
+                   for a, b in zip(results, r32))
+        fp32 = {"value": step_edges * world / (ms32 * 1e-3), "unit": UNIT, "ms_per_step": ms32, "steps": k32,
+                "kernel": sorted({layer_kernel_name(i, n, "fp32") for i, (n, _, _) in zip(info32, nets)}),
+                "same_categories_and_alive": bool(same)}
+        e32.close()
+        del e32
+
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(nets, dens, lambda i, rows: inputs[i][:rows].cpu().numpy(), kind=weight_kind(args.config))
+        # the CPU leg: the multithreaded FP32 CSR port timed as the baseline,
+        # and the FP64 oracle as the checker of this configuration
+        cpu = cpu_baseline(nets, dens, lambda i, rows: inputs[i][:rows].cpu().numpy(), weights)
+        parity = parity_check(cs, nets, prec, args.kernel, dens, weights, local, stream, inputs)
 
     clocks = clk.summary()
     if rank == 0:
@@ -437,17 +675,19 @@ def main():
             "config": {
                 "workload": workload_name(args.config, nets, prec, dens), "config": args.config,
                 "seed": SEED, "accumulate": "f32", "parallelism": f"rows sharded, {world} rank(s)",
-                "l2": "inputs larger than L2 (no flush)",
+                "l2": "L2 flushed between timed steps (256 MB write outside the events)",
                 "kernel": {0: "auto", 1: "cuda-core", 2: "tcgen05"}[args.kernel],
+                "layer_kernels": names, "layer0_kernels": l0_names,
                 "categories": [len(r["categories"]) for r in results],
                 "alive_per_layer_net0": [int(x) for x in r0["alive"][:8]],
                 "rechecked_fp64_net0": int(r0["rechecked"].sum()),
+                "parity": parity,
             },
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "fp32": fp32, "vs_fp32": (value / fp32["value"]) if fp32 else None,
             "gpu_launches": int(launches_per_run * args.steps),
         }
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.destroy_process_group()
 

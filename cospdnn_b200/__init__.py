@@ -86,6 +86,8 @@ def lib():
         L.cospdnn_engine_run_timed.argtypes = [vp, vp, f32p]
         L.cospdnn_engine_result_async.argtypes = [vp, C.c_int, vp, C.c_size_t, vp]
         L.cospdnn_engine_profile_layers.argtypes = [vp, vp, C.c_int, f32p, ip]
+        L.cospdnn_engine_net_info.argtypes = [vp, C.c_int, ip, ip, ip, vp]
+        L.cospdnn_engine_layer_values.argtypes = [vp, C.c_int, C.c_int, f32p, i32p, f32p, C.c_int64, i64p, vp]
         L.cospdnn_run_networks.argtypes = [vp, C.c_int, C.c_int, f32p]
         L.cospdnn_synth_input.argtypes = [vp, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.c_int64, C.c_double,
                                           C.c_double, C.c_int, vp]
@@ -229,6 +231,44 @@ class Engine:
                                                  out.ctypes.data_as(C.POINTER(C.c_float)),
                                                  int(max_rows), _stream(stream)))
         return out[:max_rows]
+
+    def layer_values(self, net, layer, max_rows=None, stream=None, bounds=False):
+        """Outputs of `layer` for the rows kept after it (ascending original
+        row order) and their original ids: (values [k][neuron], ids [k]),
+        plus each row's proven error bound [k] when bounds=True."""
+        info = self.nets[net]
+        if max_rows is None:
+            max_rows = info["rows"]
+        out = np.empty((max(1, max_rows), info["neuron"]), np.float32)
+        ids = np.empty(max(1, max_rows), np.int32)
+        bnd = np.empty(max(1, max_rows), np.float32)
+        cnt = C.c_int64()
+        _check(lib().cospdnn_engine_layer_values(self._h, net, int(layer),
+                                                 out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                 bnd.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 int(max_rows), C.byref(cnt), _stream(stream)))
+        k = cnt.value
+        return (out[:k], ids[:k], bnd[:k]) if bounds else (out[:k], ids[:k])
+
+    def profile_layers(self, max_iters=None, stream=None):
+        """The layer loop run eagerly with each iteration's layer kernels
+        timed by CUDA events: per-iteration milliseconds (numpy array)."""
+        if max_iters is None:
+            max_iters = max(n["layers"] for n in self.nets) + 1
+        ms = np.zeros(max_iters, np.float32)
+        it = C.c_int()
+        _check(lib().cospdnn_engine_profile_layers(self._h, _stream(stream), int(max_iters),
+                                                   ms.ctypes.data_as(C.POINTER(C.c_float)), C.byref(it)))
+        return ms[:it.value]
+
+    def net_info(self, net, stream=None):
+        """dict(kernel=KERNEL_CUDA_CORE | KERNEL_TCGEN05, row_tile=rows per
+        row tile (0: MMA tiles or row-major), layer0_counted=bool (last run))."""
+        k, t, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().cospdnn_engine_net_info(self._h, net, C.byref(k), C.byref(t), C.byref(c),
+                                             _stream(stream)))
+        return dict(kernel=k.value, row_tile=t.value, layer0_counted=bool(c.value))
 
     def launch_count(self, stream=None):
         v = C.c_int64()

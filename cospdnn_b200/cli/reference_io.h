@@ -197,7 +197,11 @@ struct Csc {
 };
 
 // Reads layer l into c; returns "" or the message of what is wrong with the
-// file (layers are read on several threads, the caller reports it).
+// file (layers are read on several threads, the caller reports it).  The
+// message prefix is the one each of the reference's readers prints: "FILE:"
+// for the images and the fuse file (src/cospdnn.cpp:21,52), "File:" for a
+// layer file (src/utils/matrix.h:277); a file that exists but cannot be read
+// takes the same prefix as its missing-file line.
 inline std::string read_layer(int neuron, int l, const std::vector<int32_t> &fuse, const std::string &dir, Csc &c) {
     const std::string name =
         dir + "/neuron" + std::to_string(neuron) + "/" + std::to_string(neuron) + "-l" + std::to_string(l + 1) + ".tsv";

@@ -220,17 +220,27 @@ __global__ void k_row_max(const uint8_t *__restrict__ src, int rows, int N, floa
     }
 }
 
-// gather of the final activations (checks only)
+// Gather of the current activations (rows 0..R-1 of the next input: the
+// output of the last computed layer for the rows kept after it) and of their
+// original ids, at most max_rows rows; for checks.
 template <typename T>
-__global__ void k_gather_final(const NetDev *__restrict__ nd_p, float *__restrict__ out, int64_t max_rows) {
+__global__ void k_gather_rows(const NetDev *__restrict__ nd_p, float *__restrict__ out, int32_t *__restrict__ ids,
+                              float *__restrict__ bounds, int64_t max_rows) {
     const NetDev &nd = *nd_p;
     const int R = nd.st->R, N = nd.N;
     const T *act = (const T *)nd.act[nd.st->in_buf];
-    const int64_t total = (int64_t)min((int64_t)R, max_rows) * N;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t rows = min((int64_t)R, max_rows), total = rows * N;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = tid; i < total; i += nth) {
         const int64_t q = i / N, j = i % N;
         out[i] = act_traits<T>::to_f(act[act_index(nd.layout, N, q, (int)j)]);
     }
+    // the row lists of the next layer: original ids, and the proven bound on
+    // |Y(fast) - Y(FP64)| of these values
+    if (ids)
+        for (int64_t q = tid; q < rows; q += nth) ids[q] = nd.orig[nd.st->layer & 1][q];
+    if (bounds)
+        for (int64_t q = tid; q < rows; q += nth) bounds[q] = nd.err[nd.st->layer & 1][q];
 }
 
 size_t elem_size(int prec) { return prec == COSPDNN_PREC_FP32 ? 4 : 2; }
@@ -1070,25 +1080,67 @@ extern "C" int cospdnn_engine_result(cospdnn_engine *e, int net, int32_t *catego
     return COSPDNN_OK;
 }
 
+namespace {
+
+// Copies rows 0..min(R, max_rows)-1 of network `net`'s current activations
+// (as floats) and their original ids (ids may be NULL) to host memory;
+// *count gets the rows copied.  Synchronizes `s`.
+int copy_current_rows(cospdnn_engine *e, int net, float *out, int32_t *ids, float *bounds, int64_t max_rows,
+                      int64_t *count, cudaStream_t s) {
+    Net &n = e->nets[net];
+    NetState st;
+    CSP_CUDA(cudaMemcpyAsync(&st, n.dev.st, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CSP_CUDA(cudaStreamSynchronize(s));
+    const int64_t rows = std::min<int64_t>(st.R, max_rows);
+    *count = rows;
+    if (rows <= 0) {
+        *count = 0;
+        return COSPDNN_OK;
+    }
+    const size_t bytes = (size_t)rows * n.d.neuron * 4;
+    float *tmp = nullptr;
+    CSP_CUDA(cudaMalloc(&tmp, bytes + 8 * rows));
+    int32_t *tids = reinterpret_cast<int32_t *>(reinterpret_cast<char *>(tmp) + bytes);
+    float *tb = reinterpret_cast<float *>(tids + rows);
+    if (n.d.precision == COSPDNN_PREC_FP32) k_gather_rows<float><<<592, 256, 0, s>>>(e->d_nets + net, tmp, tids, tb, rows);
+    else if (n.d.precision == COSPDNN_PREC_FP16) k_gather_rows<__half><<<592, 256, 0, s>>>(e->d_nets + net, tmp, tids, tb, rows);
+    else k_gather_rows<__nv_bfloat16><<<592, 256, 0, s>>>(e->d_nets + net, tmp, tids, tb, rows);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess && ids) err = cudaMemcpyAsync(ids, tids, sizeof(int32_t) * rows, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess && bounds) err = cudaMemcpyAsync(bounds, tb, sizeof(float) * rows, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    CSP_CUDA(err);
+    return COSPDNN_OK;
+}
+
+}  // namespace
+
 extern "C" int cospdnn_engine_final_values(cospdnn_engine *e, int net, float *out, int64_t max_rows,
                                            void *stream) {
     CSP_CHECK(e && out, COSPDNN_ERR_INVALID, "final_values: null argument");
     CSP_CHECK(e->built, COSPDNN_ERR_STATE, "final_values: build first");
     CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "final_values: bad net");
+    CSP_CHECK(max_rows >= 0, COSPDNN_ERR_INVALID, "final_values: negative max_rows");
     DeviceGuard g(e->device);
-    cudaStream_t s = (cudaStream_t)stream;
-    Net &n = e->nets[net];
-    const size_t bytes = (size_t)std::max<int64_t>(1, std::min<int64_t>(max_rows, n.d.rows)) * n.d.neuron * 4;
-    float *tmp = nullptr;
-    CSP_CUDA(cudaMalloc(&tmp, bytes));
-    if (n.d.precision == COSPDNN_PREC_FP32) k_gather_final<float><<<592, 256, 0, s>>>(e->d_nets + net, tmp, max_rows);
-    else if (n.d.precision == COSPDNN_PREC_FP16) k_gather_final<__half><<<592, 256, 0, s>>>(e->d_nets + net, tmp, max_rows);
-    else k_gather_final<__nv_bfloat16><<<592, 256, 0, s>>>(e->d_nets + net, tmp, max_rows);
-    cudaError_t err = cudaGetLastError();
-    if (err == cudaSuccess) err = cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToHost, s);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    cudaFree(tmp);
-    CSP_CUDA(err);
+    int64_t cnt = 0;
+    return copy_current_rows(e, net, out, nullptr, nullptr, max_rows, &cnt, (cudaStream_t)stream);
+}
+
+extern "C" int cospdnn_engine_net_info(cospdnn_engine *e, int net, int *kernel, int *row_tile,
+                                       int *layer0_counted, void *stream) {
+    CSP_CHECK(e && kernel && row_tile && layer0_counted, COSPDNN_ERR_INVALID, "net_info: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "net_info: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "net_info: bad net");
+    DeviceGuard g(e->device);
+    const Net &n = e->nets[net];
+    NetState st;
+    CSP_CUDA(cudaMemcpyAsync(&st, n.dev.st, sizeof(st), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CSP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    *kernel = n.dev.kernel;
+    *row_tile = n.dev.layout >= 2 ? n.dev.layout : 0;
+    *layer0_counted = st.l0_bits;
     return COSPDNN_OK;
 }
 
@@ -1149,12 +1201,15 @@ extern "C" int cospdnn_run_networks(const cospdnn_network *nets, int n, int devi
     return rc;
 }
 
-extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, int max_iters,
-                                             float *layer_ms, int *iters) {
-    CSP_CHECK(e && layer_ms && iters && max_iters > 0, COSPDNN_ERR_INVALID, "profile_layers: bad argument");
-    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "profile_layers: build first");
-    DeviceGuard g(e->device);
-    cudaStream_t s = (cudaStream_t)stream;
+namespace {
+
+// The layer loop of the graph run from the host, one iteration (every live
+// network advances one layer) at a time, synchronizing after each.  With
+// layer_ms the layer kernels of iteration i are timed into layer_ms[i].
+// Stops after max_iters iterations, when every network is done, or (stop_net
+// >= 0) once network stop_net has computed layer stop_layer or finished.
+int eager_run(cospdnn_engine *e, cudaStream_t s, int max_iters, float *layer_ms, int *iters, int stop_net,
+              int stop_layer) {
     int rc = take_inputs(e, s);
     if (rc) return rc;
     cudaEvent_t a, b;
@@ -1163,7 +1218,7 @@ extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, in
         const cudaError_t err = cudaEventCreate(&b);
         if (err != cudaSuccess) {
             cudaEventDestroy(a);
-            return cuda_fail(err, "profile_layers: event");
+            return cuda_fail(err, "eager run: event");
         }
     }
     rc = launch(e->k0, s);
@@ -1173,34 +1228,67 @@ extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, in
         bool live = false;
         for (size_t i = 0; i < e->nets.size() && !rc; ++i) {
             cudaError_t err = cudaMemcpyAsync(&st[i], e->nets[i].dev.st, sizeof(NetState), cudaMemcpyDeviceToHost, s);
-            if (err != cudaSuccess) rc = cuda_fail(err, "profile_layers: state copy");
+            if (err != cudaSuccess) rc = cuda_fail(err, "eager run: state copy");
         }
         if (rc) break;
         cudaError_t err = cudaStreamSynchronize(s);
-        if (err != cudaSuccess) { rc = cuda_fail(err, "profile_layers: sync"); break; }
+        if (err != cudaSuccess) { rc = cuda_fail(err, "eager run: sync"); break; }
         for (auto &x : st) live |= !x.done;
         if (!live) break;
-        cudaEventRecord(a, s);
+        if (stop_net >= 0 && (st[stop_net].done || st[stop_net].layer > stop_layer)) break;
+        if (layer_ms) cudaEventRecord(a, s);
         if (it == 0)
             for (KSpec &k : e->l0_specs) if (!rc) rc = launch(k, s);
         for (KSpec &k : e->layer_specs) if (!rc) rc = launch(k, s);
-        cudaEventRecord(b, s);
+        if (layer_ms) cudaEventRecord(b, s);
         if (!rc) rc = launch(e->k2, s);
         if (!rc) rc = launch(e->k3, s);
         if (!rc) rc = launch(e->k4_eager, s);
         if (!rc) rc = launch(e->k5, s);
         if (rc) break;
-        err = cudaEventSynchronize(b);
-        if (err != cudaSuccess) { rc = cuda_fail(err, "profile_layers: event"); break; }
-        cudaEventElapsedTime(&layer_ms[it], a, b);
+        if (layer_ms) {
+            err = cudaEventSynchronize(b);
+            if (err != cudaSuccess) { rc = cuda_fail(err, "eager run: event"); break; }
+            cudaEventElapsedTime(&layer_ms[it], a, b);
+        }
         ++it;
     }
-    *iters = it;
+    if (iters) *iters = it;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (!rc) {
         cudaError_t err = cudaStreamSynchronize(s);
-        if (err != cudaSuccess) rc = cuda_fail(err, "profile_layers: final sync");
+        if (err != cudaSuccess) rc = cuda_fail(err, "eager run: final sync");
     }
     return rc;
+}
+
+}  // namespace
+
+extern "C" int cospdnn_engine_profile_layers(cospdnn_engine *e, void *stream, int max_iters,
+                                             float *layer_ms, int *iters) {
+    CSP_CHECK(e && layer_ms && iters && max_iters > 0, COSPDNN_ERR_INVALID, "profile_layers: bad argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "profile_layers: build first");
+    DeviceGuard g(e->device);
+    return eager_run(e, (cudaStream_t)stream, max_iters, layer_ms, iters, -1, 0);
+}
+
+extern "C" int cospdnn_engine_layer_values(cospdnn_engine *e, int net, int layer, float *out, int32_t *ids,
+                                           float *bounds, int64_t max_rows, int64_t *count, void *stream) {
+    CSP_CHECK(e && out && count, COSPDNN_ERR_INVALID, "layer_values: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "layer_values: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "layer_values: bad net");
+    CSP_CHECK(layer >= 0 && layer < e->nets[net].d.layers, COSPDNN_ERR_INVALID, "layer_values: bad layer");
+    CSP_CHECK(max_rows >= 0, COSPDNN_ERR_INVALID, "layer_values: negative max_rows");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    *count = 0;
+    int rc = eager_run(e, s, e->max_layers + 1, nullptr, nullptr, net, layer);
+    if (rc) return rc;
+    NetState st;
+    CSP_CUDA(cudaMemcpyAsync(&st, e->nets[net].dev.st, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CSP_CUDA(cudaStreamSynchronize(s));
+    CSP_CHECK(st.err == 0, COSPDNN_ERR_DEVICE, "layer_values: device-side check failed");
+    if (st.layer != layer + 1) return COSPDNN_OK;  // every row was pruned before `layer`
+    return copy_current_rows(e, net, out, ids, bounds, max_rows, count, s);
 }

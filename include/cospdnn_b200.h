@@ -98,8 +98,10 @@ int cospdnn_prune_compact(const float *C, int neuron, int batch, float threshold
  * GPU that loads this library until the process exits; batch > 1048576 is
  * rejected with COSPDNN_ERR_INVALID.  The first call on a device looks up
  * that array's device address (cudaGetSymbolAddress, with the device
- * current), so make the first call on each device before any stream capture.
- * Every call clears the flags it uses; all calls share the one array, so
+ * current), so make the first call on each device before any stream capture;
+ * that address is kept for the life of the process, so the entry is not for
+ * use on a device after cudaDeviceReset (the library's module is then loaded
+ * again at a new address).  Every call clears the flags it uses; all calls share the one array, so
  * calls that overlap on the GPU (other streams, other threads) race.  No
  * cudaMalloc, cudaFree or other allocating call is made. */
 int cospdnn_prune_compact_noalloc(const float *C, int neuron, int batch, float threshold,
@@ -214,9 +216,32 @@ int cospdnn_engine_run_timed(cospdnn_engine *e, void *stream, float *ms);
 int cospdnn_engine_result(cospdnn_engine *e, int net, int32_t *categories, int64_t *count,
                           int64_t *alive_per_layer, int64_t *rechecked_per_layer, void *stream);
 /* Copies the activations of the last computed layer for the surviving rows
- * (in category order) into a host float buffer [count][neuron]; for checks. */
+ * (in category order) into a host float buffer: min(max_rows, count) rows of
+ * `neuron` floats are written (count as returned by cospdnn_engine_result;
+ * nothing is written when it is 0), so `out` needs room for
+ * min(max_rows, count) * neuron floats.  max_rows < 0 is rejected.  For checks. */
 int cospdnn_engine_final_values(cospdnn_engine *e, int net, float *out, int64_t max_rows,
                                 void *stream);
+/* Runs the layer loop eagerly (as cospdnn_engine_profile_layers) until
+ * network `net` has computed layer `layer` (0-based), then copies that
+ * layer's outputs for the rows kept after it, in ascending original-row
+ * order: min(max_rows, kept) rows of `neuron` floats into `out`, their
+ * original row ids into `ids` (may be NULL), each row's proven bound on
+ * |value - FP64 recurrence value| over its outputs into `bounds` (may be
+ * NULL; the bound behind the exact keep/prune decisions), the row count into
+ * *count (0 when every row was pruned at or before `layer`).  Replaces the reference's
+ * -DPRINT_RESULT dump of C (src/cospdnn.cu:311-320) for any layer; for checks
+ * against an FP64 recurrence.  Synchronizes `stream`. */
+int cospdnn_engine_layer_values(cospdnn_engine *e, int net, int layer, float *out, int32_t *ids,
+                                float *bounds, int64_t max_rows, int64_t *count, void *stream);
+/* What the engine resolved for network `net` at build and did in its last
+ * run: *kernel the layer kernel (COSPDNN_KERNEL_CUDA_CORE or _TCGEN05, never
+ * AUTO), *row_tile the rows per activation tile of the CUDA-core row-tile
+ * kernel (0 for the tcgen05 MMA-tile layout and the row-major gather kernel),
+ * *layer0_counted 1 when layer 0 of the last run was computed by counting
+ * the bits of a binary input.  Synchronizes `stream`. */
+int cospdnn_engine_net_info(cospdnn_engine *e, int net, int *kernel, int *row_tile,
+                            int *layer0_counted, void *stream);
 /* Number of launches of this library's kernels the last run made (device
  * counter, read after synchronizing). */
 int cospdnn_engine_launch_count(cospdnn_engine *e, int64_t *launches, void *stream);
