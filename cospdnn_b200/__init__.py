@@ -86,6 +86,8 @@ def lib():
         L.cospdnn_engine_run_timed.argtypes = [vp, vp, f32p]
         L.cospdnn_engine_result_async.argtypes = [vp, C.c_int, vp, C.c_size_t, vp]
         L.cospdnn_engine_profile_layers.argtypes = [vp, vp, C.c_int, f32p, ip]
+        L.cospdnn_engine_set_test_limits.argtypes = [vp, C.c_longlong, C.c_int, C.c_int]
+        L.cospdnn_engine_final_bound.argtypes = [vp, C.c_int, f32p, vp]
         L.cospdnn_engine_net_info.argtypes = [vp, C.c_int, ip, ip, ip, vp]
         L.cospdnn_engine_layer_values.argtypes = [vp, C.c_int, C.c_int, f32p, i32p, f32p, C.c_int64, i64p, vp]
         L.cospdnn_run_networks.argtypes = [vp, C.c_int, C.c_int, f32p]
@@ -261,6 +263,20 @@ class Engine:
         _check(lib().cospdnn_engine_profile_layers(self._h, _stream(stream), int(max_iters),
                                                    ms.ctypes.data_as(C.POINTER(C.c_float)), C.byref(it)))
         return ms[:it.value]
+
+    def set_test_limits(self, wait_cycles=0, max_iters=0, withhold_stage=0):
+        """Test hooks of the device-side failure paths (see the C header):
+        bounded-wait limit in cycles, layer-loop guard, withheld tcgen05
+        stage; all 0 restores the defaults."""
+        _check(lib().cospdnn_engine_set_test_limits(self._h, int(wait_cycles), int(max_iters),
+                                                    int(withhold_stage)))
+
+    def final_bound(self, net, stream=None):
+        """Max over the surviving rows of the proven bound on |final value -
+        FP64 recurrence value| after the last run."""
+        v = C.c_float()
+        _check(lib().cospdnn_engine_final_bound(self._h, net, C.byref(v), _stream(stream)))
+        return v.value
 
     def net_info(self, net, stream=None):
         """dict(kernel=KERNEL_CUDA_CORE | KERNEL_TCGEN05, row_tile=rows per

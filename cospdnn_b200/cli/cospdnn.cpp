@@ -3,8 +3,12 @@
 //     cospdnn.out neuron batch layer gpu_num gpu_id dataset_dir
 // Reads the dataset files (reference_io.h), runs every layer on the engine
 // (one graph launch per GPU) and prints the reference's lines
-// "layer l, feature = n" (rows alive after layer l) and
-// "Kernel Exec Time = X ms".  With gpu_num > 1 the batch is split into
+// (src/cospdnn.cu:27,262-264,302-310): "initial padding batch B",
+// per layer "layer l, feature = n" (rows alive after layer l, l <= 21),
+// "layer l, batch = b" (the kept rows padded to 128) and
+// "Layer l exec Time = t" (the layer's kernels, from a second, kernel by
+// kernel pass unless COSPDNN_LAYER_TIMES=0), then "Kernel Exec Time = X ms"
+// (the graph run).  With gpu_num > 1 the batch is split into
 // contiguous row ranges, one engine and host thread per GPU, and the counts
 // are summed.  COSPDNN_PRECISION / COSPDNN_KERNEL select precision and kernel;
 // COSPDNN_CACHE keeps parsed datasets in binary form; COSPDNN_CATEGORIES /
@@ -52,7 +56,13 @@ int main(int argc, char *argv[]) {
     std::vector<std::vector<int64_t>> alive(ng, std::vector<int64_t>(layers, 0)), rech(alive);
     std::vector<int64_t> count(ng, 0);
     std::vector<std::vector<int32_t>> cats(ng);
-    std::vector<float> ms(ng, 0.0f);
+    std::vector<float> ms(ng, 0.0f), bound(ng, 0.0f);
+    std::vector<std::vector<float>> layer_ms(ng, std::vector<float>(layers + 1, 0.0f));
+    const bool times = env_layer_times();
+    for (int g = 0; g < ng; ++g) {
+        const int64_t r0 = (int64_t)batch * g / ng, r1 = (int64_t)batch * (g + 1) / ng;
+        std::cout << "initial padding batch " << pad_tile(r1 - r0) << std::endl;
+    }
     // each worker exits the process with the reference's style of message on
     // any error (as Safe_Call does in the reference)
     auto work = [&](int g) {
@@ -68,6 +78,11 @@ int main(int argc, char *argv[]) {
               "result");
         cats[g].resize((size_t)count[g]);
         for (auto &c : cats[g]) c += r0;  // rows of the whole batch
+        check(cospdnn_engine_final_bound(e, id, &bound[g], nullptr), "final_bound");
+        if (times) {
+            int iters = 0;
+            check(cospdnn_engine_profile_layers(e, nullptr, layers + 1, layer_ms[g].data(), &iters), "profile_layers");
+        }
         cospdnn_engine_destroy(e);
     };
     if (ng == 1) {
@@ -80,9 +95,16 @@ int main(int argc, char *argv[]) {
     int64_t total = 0;
     for (int g = 0; g < ng; ++g) total += count[g];
     for (int l = 0; l < layers; ++l) {
-        int64_t f = 0;
-        for (int g = 0; g < ng; ++g) f += alive[g][l];
-        std::cout << "layer " << l << ", feature = " << f << std::endl;
+        int64_t f = 0, padded = 0;
+        float t = 0.0f;
+        for (int g = 0; g < ng; ++g) {
+            f += alive[g][l];
+            padded += pad_tile(alive[g][l]);
+            t = std::max(t, layer_ms[g][l]);
+        }
+        if (l <= 21) std::cout << "layer " << l << ", feature = " << f << std::endl;
+        std::cout << "layer " << l << ", batch = " << padded << std::endl;
+        std::cout << "Layer " << l << " exec Time = " << t << std::endl;
     }
     float tmax = 0.0f;
     for (int g = 0; g < ng; ++g) {
@@ -103,6 +125,7 @@ int main(int argc, char *argv[]) {
     rep.gpus = ng;
     for (const auto &w : net.w) rep.weights += (int64_t)w.rowidx.size();
     rep.ms = tmax;
+    for (int g = 0; g < ng; ++g) rep.dy_bound = std::max(rep.dy_bound, bound[g]);
     rep.alive.assign(layers, 0);
     rep.rechecked.assign(layers, 0);
     for (int g = 0; g < ng; ++g)

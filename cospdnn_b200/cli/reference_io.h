@@ -535,12 +535,15 @@ struct RunReport {
     int neuron = 0, batch = 0, layers = 0, precision = COSPDNN_PREC_FP16, kernel = COSPDNN_KERNEL_AUTO, gpus = 1;
     int64_t weights = 0;  // non-zeros over all layers
     float ms = 0.0f;      // device time of the run (max over GPUs)
+    float dy_bound = 0.0f;  // max proven |final value - FP64 value| over the categories
     std::vector<int64_t> alive, rechecked, categories;
 };
 
 // The result line: sizes, device time, edges = rows x non-zeros of every
-// layer and edges/s, rows alive and rows re-decided in FP64 per layer, the
-// number of categories and their hash.
+// layer and edges/s, the largest proven bound on |final value - FP64 value|
+// over the categories (the error against an FP64 recurrence of the same
+// network, as the engine tracks it), rows alive and rows re-decided in FP64
+// per layer, the number of categories and their hash.
 inline std::string json_line(const RunReport &r) {
     static const char *prec[] = {"fp32", "fp16", "bf16"};
     static const char *kern[] = {"auto", "cuda-core", "tcgen05"};
@@ -551,8 +554,8 @@ inline std::string json_line(const RunReport &r) {
     };
     const double edges = (double)r.batch * (double)r.weights;
     char num[160];
-    std::snprintf(num, sizeof num, "\"ms\": %.6g, \"edges\": %.17g, \"edges_per_s\": %.6g", (double)r.ms, edges,
-                  r.ms > 0.0f ? edges / (r.ms * 1e-3) : 0.0);
+    std::snprintf(num, sizeof num, "\"ms\": %.6g, \"edges\": %.17g, \"edges_per_s\": %.6g, \"max_abs_dy_bound\": %.6g",
+                  (double)r.ms, edges, r.ms > 0.0f ? edges / (r.ms * 1e-3) : 0.0, (double)r.dy_bound);
     char hash[40];
     std::snprintf(hash, sizeof hash, "%016llx", (unsigned long long)categories_hash(r.categories));
     std::string j = "{\"program\": \"" + r.program + "\"";
@@ -581,6 +584,22 @@ inline void report_json(const RunReport &r) {
     if (!f) die(std::string("cannot write ") + dst);
     std::fprintf(f, "%s\n", line.c_str());
     std::fclose(f);
+}
+
+// Per-layer lines of the reference's host loops (printed under its default
+// -DPRINT_TEST, src/cospdnn.cu:262-264,302-305 and src/cospdnn_double.cu:
+// 794,841,880-882): rows are padded to its 128-column tile.  It compacts
+// rows after layers 0..21 only and prints their counts there; this engine
+// compacts after every layer, so the batch line carries the padded count of
+// the rows it keeps after every layer.
+inline int64_t pad_tile(int64_t rows) { return (rows + 127) / 128 * 128; }
+
+// COSPDNN_LAYER_TIMES=0 skips the per-layer timing pass (the layer lines then
+// show 0 ms); by default the layer loop is run once more kernel by kernel to
+// time each layer's kernels, as the reference's per-layer events do.
+inline bool env_layer_times() {
+    const char *p = std::getenv("COSPDNN_LAYER_TIMES");
+    return !(p && std::string(p) == "0");
 }
 
 inline int env_precision() {

@@ -319,6 +319,7 @@ struct cospdnn_engine {
     unsigned int *finished = nullptr;
     int *loop_guard = nullptr;
     int *abort_flag = nullptr;  // raised by a layer kernel whose bounded wait expired
+    DevLimits *limits = nullptr;  // wait and loop limits read by the kernels at launch
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle loop{};
@@ -499,7 +500,7 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         }
     for (int prec : ks.tc) {
         KSpec k;
-        int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, sms);
+        int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, e->limits, sms);
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
@@ -526,7 +527,7 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         k4.grid = dim3(e->compact_ctas);
         k4.block = dim3(kCompactThreads);
         k4.arg(nets).arg(nn).arg(e->finished).arg(e->loop).arg(use_cond).arg(guard)
-            .arg(e->max_layers + 2).arg((const int *)e->abort_flag).arg(launches);
+            .arg((const DevLimits *)e->limits).arg((const int *)e->abort_flag).arg(launches);
     }
     return COSPDNN_OK;
 }
@@ -832,9 +833,14 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
     e->finished = dalloc<unsigned int>(1, e->owned);
     e->loop_guard = dalloc<int>(1, e->owned);
     e->abort_flag = dalloc<int>(1, e->owned);
-    CSP_CHECK(e->scratch && e->launches && e->finished && e->loop_guard && e->abort_flag, COSPDNN_ERR_NOMEM,
-              "build: allocation failed");
+    e->limits = dalloc<DevLimits>(1, e->owned);
+    CSP_CHECK(e->scratch && e->launches && e->finished && e->loop_guard && e->abort_flag && e->limits,
+              COSPDNN_ERR_NOMEM, "build: allocation failed");
     CSP_CUDA(cudaMemset(e->abort_flag, 0, sizeof(int)));
+    {
+        const DevLimits lim{kDefaultWaitCycles, e->max_layers + 2, 0};
+        CSP_CUDA(cudaMemcpy(e->limits, &lim, sizeof(lim), cudaMemcpyHostToDevice));
+    }
     CSP_CUDA(cudaMemset(e->finished, 0, sizeof(unsigned int)));
     CSP_CUDA(cudaMemset(e->launches, 0, sizeof(unsigned long long)));
     int rc = build_graph(e, ks);
@@ -1144,6 +1150,41 @@ extern "C" int cospdnn_engine_net_info(cospdnn_engine *e, int net, int *kernel, 
     return COSPDNN_OK;
 }
 
+extern "C" int cospdnn_engine_final_bound(cospdnn_engine *e, int net, float *max_bound, void *stream) {
+    CSP_CHECK(e && max_bound, COSPDNN_ERR_INVALID, "final_bound: null argument");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "final_bound: build first");
+    CSP_CHECK(net >= 0 && net < (int)e->nets.size(), COSPDNN_ERR_INVALID, "final_bound: bad net");
+    DeviceGuard g(e->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const Net &n = e->nets[net];
+    NetState st;
+    CSP_CUDA(cudaMemcpyAsync(&st, n.dev.st, sizeof(st), cudaMemcpyDeviceToHost, s));
+    CSP_CUDA(cudaStreamSynchronize(s));
+    *max_bound = 0.0f;
+    if (st.R <= 0) return COSPDNN_OK;
+    std::vector<float> b((size_t)st.R);
+    CSP_CUDA(cudaMemcpyAsync(b.data(), n.dev.err[st.layer & 1], sizeof(float) * st.R, cudaMemcpyDeviceToHost, s));
+    CSP_CUDA(cudaStreamSynchronize(s));
+    for (float x : b) *max_bound = std::max(*max_bound, x);
+    return COSPDNN_OK;
+}
+
+extern "C" int cospdnn_engine_set_test_limits(cospdnn_engine *e, long long wait_cycles, int max_iters,
+                                              int withhold_stage) {
+    CSP_CHECK(e, COSPDNN_ERR_INVALID, "set_test_limits: null engine");
+    CSP_CHECK(e->built, COSPDNN_ERR_STATE, "set_test_limits: build first");
+    CSP_CHECK(wait_cycles >= 0 && max_iters >= 0 && (withhold_stage == 0 || withhold_stage == 1), COSPDNN_ERR_INVALID,
+              "set_test_limits: bad argument");
+    CSP_CHECK(wait_cycles == 0 || wait_cycles >= 1000000, COSPDNN_ERR_INVALID,
+              "set_test_limits: a wait limit below 1e6 cycles would fail correct runs");
+    DeviceGuard g(e->device);
+    const DevLimits lim{wait_cycles ? wait_cycles : kDefaultWaitCycles, max_iters ? max_iters : e->max_layers + 2,
+                        withhold_stage};
+    CSP_CUDA(cudaDeviceSynchronize());  // no run in flight reads the old limits
+    CSP_CUDA(cudaMemcpy(e->limits, &lim, sizeof(lim), cudaMemcpyHostToDevice));
+    return COSPDNN_OK;
+}
+
 extern "C" int cospdnn_engine_launch_count(cospdnn_engine *e, int64_t *launches, void *stream) {
     CSP_CHECK(e && launches, COSPDNN_ERR_INVALID, "launch_count: null argument");
     CSP_CHECK(e->built, COSPDNN_ERR_STATE, "launch_count: build first");
@@ -1233,8 +1274,12 @@ int eager_run(cospdnn_engine *e, cudaStream_t s, int max_iters, float *layer_ms,
         if (rc) break;
         cudaError_t err = cudaStreamSynchronize(s);
         if (err != cudaSuccess) { rc = cuda_fail(err, "eager run: sync"); break; }
-        for (auto &x : st) live |= !x.done;
-        if (!live) break;
+        bool failed = false;
+        for (auto &x : st) {
+            live |= !x.done;
+            failed |= x.err != 0;  // a device-side check stopped the run (as the graph's loop stops)
+        }
+        if (!live || failed) break;
         if (stop_net >= 0 && (st[stop_net].done || st[stop_net].layer > stop_layer)) break;
         if (layer_ms) cudaEventRecord(a, s);
         if (it == 0)

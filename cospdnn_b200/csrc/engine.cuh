@@ -116,6 +116,17 @@ struct NetDev {
 
 enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
 
+// Limits of the device-side waits and of the layer loop, in engine memory and
+// read by the kernels at every launch (cospdnn_engine_set_test_limits changes
+// them between runs so that tests can make a bounded wait or the loop guard
+// run out and check the error path).
+struct DevLimits {
+    long long wait_cycles;  // bounded mbarrier waits of k_layer_tc (SM clock cycles)
+    int max_iters;          // layer-loop iterations before the guard stops the run
+    int withhold_stage;     // 1: CTA 0 of k_layer_tc issues no copy for its first stage
+};
+constexpr long long kDefaultWaitCycles = 4000000000LL;  // about 2 s at 1.9 GHz
+
 // Rows per compaction chunk (one CTA of k_compact; a multiple of 32).
 constexpr int kCompactChunk = 1024;
 

@@ -325,7 +325,7 @@ constexpr int kCompactThreads = kCompactChunk;
 
 __global__ void __launch_bounds__(kCompactThreads)
     k_compact(const NetDev *__restrict__ nets, int nnets, unsigned int *finished_ctas,
-              cudaGraphConditionalHandle loop, int use_cond, int *loop_guard, int max_iters,
+              cudaGraphConditionalHandle loop, int use_cond, int *loop_guard, const DevLimits *__restrict__ limits,
               const int *abort_flag, unsigned long long *launches) {
     count_launch(launches);
     __shared__ int red[kCompactThreads / 32];
@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(kCompactThreads)
         int live = 0;
         for (int i = 0; i < nnets; ++i) live |= !(*(volatile int *)&nets[i].st->done);
         const int it = ++*loop_guard;
-        if (it > max_iters || *(volatile const int *)abort_flag) {
+        if (it > limits->max_iters || *(volatile const int *)abort_flag) {
             for (int i = 0; i < nnets; ++i) nets[i].st->err = COSPDNN_ERR_DEVICE;
             live = 0;
         }

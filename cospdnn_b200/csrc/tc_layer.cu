@@ -52,7 +52,6 @@ constexpr int kMmaWarp = 1;
 constexpr int kEpiWarps = 4;  // warps 2..5: (warp & 3) covers the four TMEM lane quarters
 constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr int kTmemCols = kChunk * 16;      // 512: one accumulator per chunk column
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
 struct __align__(128) TcSmem {
     uint8_t stage[kStages][kStageBytes];
@@ -63,6 +62,7 @@ struct __align__(128) TcSmem {
     unsigned long long fin;
     uint32_t tmem_base;
     volatile int abort;
+    long long wait_cycles;  // limit of every wait of this launch (DevLimits)
 };
 constexpr size_t kSmemBytes = sizeof(TcSmem) + 128;
 static_assert(kSmemBytes <= 227 * 1024, "tcgen05 layer kernel shared memory");
@@ -88,7 +88,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, uint32_t parity
     const long long t0 = clock64();
     while (!mbar_try_wait(b, parity)) {
         if (sm.abort) return false;
-        if (clock64() - t0 > kWaitCycles) {
+        if (clock64() - t0 > sm.wait_cycles) {
             sm.abort = 1;
             return false;
         }
@@ -218,7 +218,7 @@ __device__ __forceinline__ void epilogue_cols(const float *v, int ncol, float bi
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 1)
     k_layer_tc(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches,
-               int *abort_flag) {
+               int *abort_flag, const DevLimits *__restrict__ limits) {
     count_launch(launches);
     const int64_t total = tc_items(nets, nnets, prec);
     if (total == 0 || blockIdx.x >= total) return;  // uniform across the CTA
@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(&sm.tempty, kEpiWarps * 32);
         mbar_init(&sm.fin, 1);
         sm.abort = 0;
+        sm.wait_cycles = limits->wait_cycles;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == kMmaWarp) {
@@ -253,6 +254,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             uint32_t fill = 0;
             bool ok = true;
+            // test hook: CTA 0 issues nothing for its first stage, so the MMA
+            // issuer's bounded wait on it runs out (the error path of a lost copy)
+            const bool withhold = limits->withhold_stage != 0 && blockIdx.x == 0;
             for (int64_t idx = blockIdx.x; idx < total && ok; idx += gridDim.x) {
                 const Item it = tc_item(nets, nnets, prec, idx);
                 const NetDev &nd = nets[it.net];
@@ -265,6 +269,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const int4 st = lw.tc_stage[q];  // a_first, a_count, b_first, n_mma
                     const uint32_t s = fill % kStages, u = fill / kStages;
                     if (u > 0 && !mbar_wait(&sm.empty[s], (u - 1) & 1, sm)) { ok = false; break; }
+                    if (withhold && fill == 0) {
+                        ++fill;
+                        continue;
+                    }
                     const uint32_t base = smem_u32(sm.stage[s]);
                     const uint32_t code_bytes = (uint32_t)((st.w + 7) & ~7) * 2;
                     mbar_expect_tx(&sm.full[s], (uint32_t)st.y * kTileBytes + (uint32_t)st.w * kBBytes + code_bytes);
@@ -279,8 +287,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             // wait (bounded) for the last fill of every stage
             const uint32_t first = fill > (uint32_t)kStages ? fill - kStages : 0u;
             for (uint32_t f = first; f < fill; ++f) {
+                if (withhold && f == 0) continue;  // nothing was issued for it
                 const long long t0 = clock64();
-                while (!mbar_try_wait(&sm.full[f % kStages], (f / kStages) & 1) && clock64() - t0 < kWaitCycles) {
+                while (!mbar_try_wait(&sm.full[f % kStages], (f / kStages) & 1) && clock64() - t0 < sm.wait_cycles) {
                 }
             }
         }
@@ -327,7 +336,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             // every MMA this thread issued has completed before TMEM is freed
             mma_commit(&sm.fin);
             const long long t0 = clock64();
-            while (!mbar_try_wait(&sm.fin, 0) && clock64() - t0 < kWaitCycles) {
+            while (!mbar_try_wait(&sm.fin, 0) && clock64() - t0 < sm.wait_cycles) {
             }
         }
         __syncwarp();
@@ -503,13 +512,13 @@ int tc_build_blocks(const std::vector<int32_t> &colptr, const std::vector<int32_
 }
 
 int tc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, unsigned long long *launches, int *abort_flag,
-                  int sms) {
+                  const DevLimits *limits, int sms) {
     k.fn = prec == COSPDNN_PREC_BF16 ? (void *)k_layer_tc<__nv_bfloat16> : (void *)k_layer_tc<__half>;
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
     k.grid = dim3(sms);  // one CTA (all of TMEM) per SM
     k.block = dim3(kThreads);
     k.smem = kSmemBytes;
-    k.arg(nets).arg(nnets).arg(prec).arg(launches).arg(abort_flag);
+    k.arg(nets).arg(nnets).arg(prec).arg(launches).arg(abort_flag).arg(limits);
     return COSPDNN_OK;
 }
 

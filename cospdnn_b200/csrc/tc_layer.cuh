@@ -15,6 +15,6 @@ int tc_build_blocks(const std::vector<int32_t> &colptr, const std::vector<int32_
                     std::vector<void *> &owned);
 // Launch description of the layer kernel for the tcgen05 nets of precision `prec`.
 int tc_layer_spec(KSpec &spec, NetDev *nets, int nnets, int prec, unsigned long long *launches,
-                  int *abort_flag, int sms);
+                  int *abort_flag, const DevLimits *limits, int sms);
 
 }  // namespace cospdnn

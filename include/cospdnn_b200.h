@@ -234,6 +234,12 @@ int cospdnn_engine_final_values(cospdnn_engine *e, int net, float *out, int64_t 
  * against an FP64 recurrence.  Synchronizes `stream`. */
 int cospdnn_engine_layer_values(cospdnn_engine *e, int net, int layer, float *out, int32_t *ids,
                                 float *bounds, int64_t max_rows, int64_t *count, void *stream);
+/* Largest of the surviving rows' proven bounds on |final value - FP64
+ * recurrence value| after the last run (0 when no row survived): the
+ * maximum error of the result against an FP64 oracle of the same
+ * recurrence, as the engine tracks it to decide every row exactly.
+ * Synchronizes `stream`. */
+int cospdnn_engine_final_bound(cospdnn_engine *e, int net, float *max_bound, void *stream);
 /* What the engine resolved for network `net` at build and did in its last
  * run: *kernel the layer kernel (COSPDNN_KERNEL_CUDA_CORE or _TCGEN05, never
  * AUTO), *row_tile the rows per activation tile of the CUDA-core row-tile
@@ -242,6 +248,22 @@ int cospdnn_engine_layer_values(cospdnn_engine *e, int net, int layer, float *ou
  * the bits of a binary input.  Synchronizes `stream`. */
 int cospdnn_engine_net_info(cospdnn_engine *e, int net, int *kernel, int *row_tile,
                             int *layer0_counted, void *stream);
+/* Test hooks for the device-side failure paths (no counterpart in the
+ * reference, whose Safe_Call exits the process, src/gpu_lib/gpu_runtime.h:6-17).
+ * Every wait in the engine's kernels is bounded and the layer loop has an
+ * iteration guard; when one runs out the run stops and
+ * cospdnn_engine_result returns COSPDNN_ERR_DEVICE, and the next run starts
+ * clean.  These set, for the following runs: wait_cycles, the limit of each
+ * bounded wait of the tcgen05 layer kernel in SM clock cycles (0 = the
+ * default of 4e9, about 2 s; values below 1e6 are rejected); max_iters, the
+ * layer-loop iterations after which the guard stops the run (0 = the default
+ * of the deepest network's layers + 2); withhold_stage = 1 makes the first
+ * block of the tcgen05 layer kernel skip the copies of its first stage, so
+ * that its wait for them runs out (a copy that never arrives, made on
+ * purpose; no fault, no hang).  (0, 0, 0) restores the defaults.
+ * Synchronizes the device. */
+int cospdnn_engine_set_test_limits(cospdnn_engine *e, long long wait_cycles, int max_iters,
+                                   int withhold_stage);
 /* Number of launches of this library's kernels the last run made (device
  * counter, read after synchronizing). */
 int cospdnn_engine_launch_count(cospdnn_engine *e, int64_t *launches, void *stream);

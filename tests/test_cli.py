@@ -136,6 +136,14 @@ def _alive(text, prefix):
     return [got[k] for k in sorted(got)]
 
 
+def _per_layer(text, pat):
+    return {int(m.group(1)): m.group(2) for m in re.finditer(pat, text)}
+
+
+def _pad(n):
+    return (int(n) + 127) // 128 * 128
+
+
 @pytest.mark.gpu
 def test_cli_single_matches_oracle(tmp_path):
     torch = pytest.importorskip("torch")
@@ -154,6 +162,11 @@ def test_cli_single_matches_oracle(tmp_path):
                              capture_output=True, text=True, timeout=600, env=env)
         assert out.returncode == 0, out.stdout + out.stderr
         assert _alive(out.stdout, "") == list(ref["alive"])
+        assert "initial padding batch 512" in out.stdout
+        batch = _per_layer(out.stdout, r"layer (\d+), batch = (\d+)")
+        assert [int(batch[l]) for l in range(6)] == [_pad(a) for a in ref["alive"]]
+        times = _per_layer(out.stdout, r"Layer (\d+) exec Time = ([0-9.e+-]+)\n")
+        assert sorted(times) == list(range(6)) and float(times[0]) > 0
         assert "Kernel Exec Time = " in out.stdout
         assert f"[Categories] :{len(ref['categories'])}" in out.stdout
         assert "categories check: PASS" in out.stdout
@@ -164,6 +177,37 @@ def test_cli_single_matches_oracle(tmp_path):
     out = subprocess.run([_exe("cospdnn"), "1024", "500", "6", "1", "0", str(tmp_path)],
                          capture_output=True, text=True, timeout=600, env=env)
     assert out.returncode == 2 and "categories check: FAIL" in out.stdout and "extra 1" in out.stdout
+
+
+@pytest.mark.gpu
+def test_cli_layer_lines_past_layer_21(tmp_path):
+    """The reference prints "feature" lines for the layers it compacts
+    (l <= 21) and "batch" / "exec Time" lines for every layer
+    (src/cospdnn.cu:262-264,302-305); the JSON line carries the proven bound
+    on |final value - FP64 value|."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import json
+    ref = _dataset(tmp_path, 1024, 24, 300, 59, 0)
+    assert ref["alive"][-1] > 0
+    env = dict(os.environ, COSPDNN_JSON="1")
+    out = subprocess.run([_exe("cospdnn"), "1024", "300", "24", "1", "0", str(tmp_path)],
+                         capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert _alive(out.stdout, "") == list(ref["alive"][:22])
+    assert "layer 22, feature" not in out.stdout
+    batch = _per_layer(out.stdout, r"layer (\d+), batch = (\d+)")
+    assert [int(batch[l]) for l in range(24)] == [_pad(a) for a in ref["alive"]]
+    times = _per_layer(out.stdout, r"Layer (\d+) exec Time = ([0-9.e+-]+)\n")
+    assert sorted(times) == list(range(24)) and all(float(times[l]) > 0 for l in range(24))
+    line = json.loads([x for x in out.stdout.splitlines() if x.startswith("{")][0])
+    assert line["alive"] == list(ref["alive"]) and line["max_abs_dy_bound"] >= 0
+    # without the timing pass the exec Time lines read 0
+    env["COSPDNN_LAYER_TIMES"] = "0"
+    out = subprocess.run([_exe("cospdnn"), "1024", "300", "24", "1", "0", str(tmp_path)],
+                         capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0 and "Layer 23 exec Time = 0\n" in out.stdout
 
 
 @pytest.mark.gpu
@@ -184,6 +228,12 @@ def test_cli_double_matches_oracle(tmp_path):
     assert out.returncode == 0, out.stdout + out.stderr
     assert _alive(out.stdout, "SpDNN 1 ") == list(ref1["alive"])
     assert _alive(out.stdout, "SpDNN 2 ") == list(ref2["alive"])
+    assert "initial padding batch 512 and 384" in out.stdout
+    batch = {int(m.group(1)): (int(m.group(2)), int(m.group(3)))
+             for m in re.finditer(r"layer (\d+), batch1 = (\d+), batch2 = (\d+)", out.stdout)}
+    a1 = list(ref1["alive"]) + [0, 0]
+    assert [batch[l] for l in range(7)] == [(_pad(a1[l]), _pad(ref2["alive"][l])) for l in range(7)]
+    assert len(re.findall(r"Layer \d+ exec Time = [0-9.e+-]+ms", out.stdout)) == 7
     assert "Total Kernel Exec Time = " in out.stdout
     assert "SpDNN 1 categories check: PASS" in out.stdout and "SpDNN 2 categories check: PASS" in out.stdout
     assert cat.read(tmp_path / "ours2.tsv").tolist() == list(ref2["categories"])
