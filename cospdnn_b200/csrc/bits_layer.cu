@@ -410,6 +410,56 @@ __global__ void k_convert_bits(const uint8_t *__restrict__ src, int rows, int N,
     }
 }
 
+// Bit planes of packed-bit rows (COSPDNN_INPUT_BITS) with the row maxima:
+// one CTA per unit of 32 rows.  The unit's rows are read a slice of up to
+// kConvSlice 32-feature words at a time with coalesced 4-byte loads into
+// shared memory (row stride padded by one word, so that lane r reading row
+// r of a column hits bank r); each warp then takes word columns of the
+// slice: lane r reads row r's word, the warp transposes the 32x32 bit block
+// and writes one 128-byte line of bit planes.  A row's maximum is 1 when any
+// of its bits is set.
+constexpr int kConvThreads = 256;
+constexpr int kConvSlice = 256;  // words per row staged at once (32 KB of shared memory)
+
+__global__ void __launch_bounds__(kConvThreads)
+    k_convert_packed(const uint8_t *__restrict__ src, int rows, int N, uint32_t *__restrict__ bits,
+                     float *__restrict__ err0, float *__restrict__ mx0) {
+    __shared__ uint32_t cs[32 * (kConvSlice + 1)];
+    __shared__ uint32_t s_any[32];
+    const int wpr = N / 32;  // 32-feature words per row
+    const int units = (rows + 31) / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int r0 = u * 32, nr = min(32, rows - r0);
+        __syncthreads();  // the previous unit is done with s_any
+        if (threadIdx.x < 32) s_any[threadIdx.x] = 0u;
+        // N % 32 == 0, so rows of N/8 bytes are whole words and every row
+        // starts on a word boundary (the input is 16-byte aligned)
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(src + (int64_t)r0 * (N / 8));
+        uint32_t any = 0u;
+        for (int c0 = 0; c0 < wpr; c0 += kConvSlice) {
+            const int sw = min(kConvSlice, wpr - c0), stride = sw + 1;
+            __syncthreads();  // the previous slice is done with cs
+            for (int i = threadIdx.x; i < 32 * sw; i += kConvThreads) {
+                const int r = i / sw, c = i - r * sw;
+                cs[r * stride + c] = r < nr ? __ldg(w + (int64_t)r * wpr + c0 + c) : 0u;
+            }
+            __syncthreads();
+            for (int c = warp; c < sw; c += kConvThreads / 32) {
+                const uint32_t x = cs[lane * stride + c];
+                any |= x;
+                bits[(int64_t)u * N + (int64_t)(c0 + c) * 32 + lane] = transpose32(x, lane);
+            }
+        }
+        if (any) atomicOr(&s_any[lane], 1u);
+        __syncthreads();
+        if (threadIdx.x < nr) {
+            err0[r0 + threadIdx.x] = 0.0f;
+            mx0[r0 + threadIdx.x] = s_any[threadIdx.x] ? 1.0f : 0.0f;
+        }
+    }
+}
+
 }  // namespace
 
 int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx, const std::vector<float> &vals,
@@ -562,9 +612,14 @@ void l0_convert_bits(const uint8_t *src, int format, int rows, int N, uint32_t *
                      int *nonbin, cudaStream_t s) {
     const int64_t warps = (rows + 31) / 32;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warps + 7) / 8, 148 * 16));
-    if (format == COSPDNN_INPUT_BITS)
-        k_convert_bits<COSPDNN_INPUT_BITS><<<blocks, 256, 0, s>>>(src, rows, N, bits, err0, mx0, nonbin);
-    else k_convert_bits<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, rows, N, bits, err0, mx0, nonbin);
+    if (format == COSPDNN_INPUT_BITS) {
+        // packed bits are binary by construction: the flag stays clear
+        const int units = (rows + 31) / 32;
+        k_convert_packed<<<(int)std::max(1, std::min(units, 148 * 8)), kConvThreads, 0, s>>>(src, rows, N, bits,
+                                                                                            err0, mx0);
+    } else {
+        k_convert_bits<COSPDNN_INPUT_U8><<<blocks, 256, 0, s>>>(src, rows, N, bits, err0, mx0, nonbin);
+    }
 }
 
 }  // namespace cospdnn

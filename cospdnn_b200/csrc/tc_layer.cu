@@ -60,6 +60,7 @@ struct __align__(128) TcSmem {
     unsigned long long tfull;
     unsigned long long tempty;
     unsigned long long fin;
+    int nmma[kStages];  // MMAs of the stage in each slot, written by the producer before its copies
     uint32_t tmem_base;
     volatile int abort;
     long long wait_cycles;  // limit of every wait of this launch (DevLimits)
@@ -98,8 +99,10 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, uint32_t parity
 __device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
+// (release: the producer's shared-memory writes before it are seen by a
+// thread whose wait on the barrier completes)
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
 }
 // Bulk copy global -> this CTA's shared memory, completing on `bar` (no multicast).
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, unsigned long long *bar) {
@@ -265,14 +268,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const char *in = (const char *)(l == 0 ? nd.y0 : nd.act[nd.st->in_buf]);
                 const char *tile = in + (int64_t)it.tile * (N / 16) * kTileBytes;
                 const int s0 = lw.tc_chunk_ptr[it.chunk], s1 = lw.tc_chunk_ptr[it.chunk + 1];
+                // stage descriptors a_first, a_count, b_first, n_mma; the next
+                // one is loaded before this one's slot is waited for, so its
+                // latency overlaps the wait and the copies
+                int4 next = s0 < s1 ? lw.tc_stage[s0] : make_int4(0, 0, 0, 0);
                 for (int q = s0; q < s1; ++q) {
-                    const int4 st = lw.tc_stage[q];  // a_first, a_count, b_first, n_mma
+                    const int4 st = next;
+                    if (q + 1 < s1) next = lw.tc_stage[q + 1];
                     const uint32_t s = fill % kStages, u = fill / kStages;
                     if (u > 0 && !mbar_wait(&sm.empty[s], (u - 1) & 1, sm)) { ok = false; break; }
                     if (withhold && fill == 0) {
                         ++fill;
                         continue;
                     }
+                    sm.nmma[s] = st.w;  // read by the MMA issuer after its wait on full[s]
                     const uint32_t base = smem_u32(sm.stage[s]);
                     const uint32_t code_bytes = (uint32_t)((st.w + 7) & ~7) * 2;
                     mbar_expect_tx(&sm.full[s], (uint32_t)st.y * kTileBytes + (uint32_t)st.w * kBBytes + code_bytes);
@@ -308,9 +317,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc_fence_after();
                 const int s0 = lw.tc_chunk_ptr[it.chunk], s1 = lw.tc_chunk_ptr[it.chunk + 1];
                 for (int q = s0; q < s1; ++q) {
-                    const int n_mma = lw.tc_stage[q].w;
                     const uint32_t s = fill % kStages, u = fill / kStages;
                     if (!mbar_wait(&sm.full[s], u & 1, sm)) { ok = false; break; }
+                    const int n_mma = sm.nmma[s];
                     const uint32_t base = smem_u32(sm.stage[s]);
                     const uint64_t adesc0 = smem_desc(base), bdesc0 = smem_desc(base + kStageA);
                     const uint4 *code8 = reinterpret_cast<const uint4 *>(sm.stage[s] + kStageA + kStageB);
