@@ -448,129 +448,98 @@ __global__ void __launch_bounds__(kCompactThreads)
 // ---- K5: move the kept rows to the front of the next input buffer ---------
 // Row q of act[in_buf] <- row cmap[q] of act[in_buf ^ 1].
 // Row-major and MMA-tile nets: 16-byte pieces (row-major: consecutive; MMA
-// tiles: the two 8-feature halves of each block).  Row-tile nets: one CTA per
-// destination tile; the source tiles its rows come from (a contiguous range,
-// the map being increasing) are staged in shared memory a feature chunk at a
-// time with 16-byte loads, and the destination tile is written contiguously
-// (rows past the kept count are zero).
+// tiles: the two 8-feature halves of each block).  Row-tile nets: one CTA
+// per destination tile, see copy_tile.
 constexpr int kCopyThreads = 256;
-constexpr int kCopyStageBytes = 40 * 1024;
 
-// Copies `pieces` U-sized pieces from global to shared memory, 8 in flight
-// per thread.
-template <typename U>
-__device__ __forceinline__ void stage_pieces(U *to, const U *__restrict__ from, int pieces) {
-    int k = threadIdx.x;
-    for (; k + 7 * kCopyThreads < pieces; k += 8 * kCopyThreads) {
-        U v[8];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) v[t] = __ldg(from + k + t * kCopyThreads);
-#pragma unroll
-        for (int t = 0; t < 8; ++t) to[k + t * kCopyThreads] = v[t];
-    }
-    for (; k < pieces; k += kCopyThreads) to[k] = __ldg(from + k);
-}
-
-// One destination row tile; U = the piece type of one feature column when a
-// column is 8 or 16 bytes (columns of 32 bytes and more use 16-byte pieces).
-constexpr int kCopyFeatures = 64;  // fewest features per work item of a row-tile copy
-
-// Feature chunks per destination tile of a row-tile copy: enough items for
-// about two per CTA of the grid, chunks of at least kCopyFeatures.
-__device__ __forceinline__ int copy_chunks(const NetDev &nd, int grid) {
-    const int tiles = (nd.st->copy_R + nd.layout - 1) / nd.layout;
-    const int most = (nd.N + kCopyFeatures - 1) / kCopyFeatures;
-    if (tiles == 0) return 1;
-    return max(1, min(most, (2 * grid + tiles - 1) / tiles));
-}
+// Row-tile copy of destination tile q of one net (a CTA's work item): rows
+// q*TR .. q*TR+TR-1 of the next input <- the kept output rows cmap[...],
+// rows past the kept count zero.  The tile's row map is read once into
+// shared memory; threads then take the tile's feature columns in turn.
+// Kept rows are increasing, so a tile's rows come from a few consecutive
+// source tiles: when a feature column is one 8- or 16-byte piece, each
+// distinct source column is loaded once (one vector load, coalesced across
+// the threads of consecutive features) and the values are picked out of it;
+// wider columns move 16-byte destination pieces whose values are loaded one
+// by one (repeats hit L1).
+constexpr int kCopyMaxTR = 128;
 
 template <typename E>
-__device__ __forceinline__ void copy_tile(const NetDev &nd, int tq, int fbeg, int fend, uint4 *stage) {
-    // s_src[k]: the k-th distinct source tile of this tile's rows (the map is
-    // increasing, so they come in order); row r reads slot s_tile[r], row
-    // s_off[r] of it (s_tile = -1: past the kept rows)
-    __shared__ int s_tile[128], s_off[128], s_src[128], s_raw[128];
-    const int N = nd.N, TR = nd.layout, ib = nd.st->in_buf, R = nd.st->copy_R;
+__device__ __forceinline__ void copy_tile(const NetDev &nd, int q, int *s_map) {
+    constexpr int kV = 16 / (int)sizeof(E);  // values of a 16-byte piece
+    const int TR = nd.layout, N = nd.N, R = nd.st->copy_R, ib = nd.st->in_buf;
+    const int lg = __ffs(TR) - 1;            // TR is a power of two
+    const int colb = TR * (int)sizeof(E);    // bytes of a feature column
     const E *src = (const E *)nd.act[ib ^ 1];
-    E *dst = (E *)nd.act[ib] + (int64_t)tq * N * TR;
-    __syncthreads();  // the previous tile is done with the shared arrays
+    E *dst = (E *)nd.act[ib] + ((int64_t)q * N << lg);
+    __syncthreads();  // the previous tile is done with s_map
     for (int r = threadIdx.x; r < TR; r += blockDim.x) {
-        const int q = tq * TR + r;
-        const int p = q < R ? nd.cmap[q] : -1;
-        s_raw[r] = p < 0 ? -1 : p / TR;
-        s_off[r] = p < 0 ? 0 : p % TR;
+        const int row = q * TR + r;
+        s_map[r] = row < R ? nd.cmap[row] : -1;
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < TR; r += blockDim.x) {
-        const int t = s_raw[r];
-        int rank = -1;
-        if (t >= 0) {
-            rank = 0;
-            for (int k = 1; k <= r; ++k) rank += s_raw[k] != s_raw[k - 1];
-            if (r == 0 || s_raw[r - 1] != t) s_src[rank] = t;
-        }
-        s_tile[r] = rank;
-    }
-    __syncthreads();
-    int nsrc = 0;
-    for (int r = 0; r < TR; ++r) nsrc = max(nsrc, s_tile[r] + 1);
-    const int colb = TR * (int)sizeof(E);  // bytes of a feature column: 8 or a multiple of 16
-    const int fc_max = kCopyStageBytes / (nsrc * colb);
-    const E *sst = (const E *)stage;
-    if (fc_max == 0) {
-        // one feature column of every source tile does not fit: gather directly
-        for (int i = fbeg * TR + threadIdx.x; i < fend * TR; i += blockDim.x) {
-            const int f = i / TR, r = i - f * TR, t = s_tile[r];
-            dst[i] = t >= 0 ? src[((int64_t)s_src[t] * N + f) * TR + s_off[r]] : E(0);
+    if (colb == 16 || colb == 8) {
+        // TR <= 8 values per column: the map in registers
+        int pm[kV];
+#pragma unroll
+        for (int i = 0; i < kV; ++i) pm[i] = i < TR ? s_map[i] : -1;
+        for (int f = threadIdx.x; f < N; f += blockDim.x) {
+            __align__(16) E v[kV];
+            int64_t cur = -1;
+            uint4 col = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+            for (int i = 0; i < kV; ++i) {
+                v[i] = E(0);
+                const int p = pm[i];
+                if (p < 0) continue;
+                const int64_t t = p >> lg;
+                if (t != cur) {
+                    cur = t;
+                    const E *c = src + ((t * N + f) << lg);
+                    if (colb == 16) {
+                        col = __ldg(reinterpret_cast<const uint4 *>(c));
+                    } else {
+                        const uint2 h = __ldg(reinterpret_cast<const uint2 *>(c));
+                        col = make_uint4(h.x, h.y, 0u, 0u);
+                    }
+                }
+                const int off = (p & (TR - 1)) * (int)sizeof(E);  // byte offset in the column
+                const uint32_t w = off < 8 ? (off < 4 ? col.x : col.y) : (off < 12 ? col.z : col.w);
+                if (sizeof(E) == 4) {
+                    v[i] = *reinterpret_cast<const E *>(&w);
+                } else {
+                    const uint16_t h = (uint16_t)(w >> (8 * (off & 3)));
+                    v[i] = *reinterpret_cast<const E *>(&h);
+                }
+            }
+            if (colb == 16) *reinterpret_cast<uint4 *>(dst + ((int64_t)f << lg)) = *reinterpret_cast<const uint4 *>(v);
+            else *reinterpret_cast<uint2 *>(dst + ((int64_t)f << lg)) = *reinterpret_cast<const uint2 *>(v);
         }
         return;
     }
-    for (int f0 = fbeg; f0 < fend; f0 += fc_max) {
-        const int fc = min(fc_max, fend - f0);
-        for (int sidx = 0; sidx < nsrc; ++sidx) {
-            const E *from = src + ((int64_t)s_src[sidx] * N + f0) * TR;
-            E *to = (E *)stage + (int64_t)sidx * fc_max * TR;
-            if (colb == 8)
-                stage_pieces(reinterpret_cast<uint2 *>(to), reinterpret_cast<const uint2 *>(from), fc);
-            else
-                stage_pieces(reinterpret_cast<uint4 *>(to), reinterpret_cast<const uint4 *>(from), fc * colb / 16);
-        }
-        __syncthreads();
-        {
-            // destination columns in 16-byte pieces (one 8-byte piece for an
-            // 8-byte column): kV consecutive rows of one feature per store
-            constexpr int kV = 16 / (int)sizeof(E);
-            const int pcs = colb >= 16 ? colb / 16 : 1;  // pieces per feature
-            for (int u = threadIdx.x; u < fc * pcs; u += kCopyThreads) {
-                const int fl = u / pcs, r0 = (u - fl * pcs) * kV;
-                __align__(16) E col[kV];
+    // wider columns: 16-byte destination pieces, P per column (a power of two)
+    const int lp = lg - (__ffs(kV) - 1);  // log2 of pieces per column
+    const int total = N << lp;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        const int f = u >> lp, pc = u & ((1 << lp) - 1);
+        __align__(16) E v[kV];
 #pragma unroll
-                for (int v = 0; v < kV; ++v) {
-                    const int r = r0 + v;
-                    const int t = r < TR ? s_tile[r] : -1;
-                    col[v] = t >= 0 ? sst[(int64_t)t * fc_max * TR + fl * TR + s_off[r]] : E(0);
-                }
-                E *d = dst + (int64_t)(f0 + fl) * TR + r0;
-                if (colb >= 16) *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(col);
-                else *reinterpret_cast<uint2 *>(d) = *reinterpret_cast<const uint2 *>(col);
-            }
+        for (int i = 0; i < kV; ++i) {
+            const int p = s_map[pc * kV + i];
+            v[i] = p < 0 ? E(0) : src[(((int64_t)(p >> lg) * N + f) << lg) + (p & (TR - 1))];
         }
-        __syncthreads();
+        *reinterpret_cast<uint4 *>(dst + ((int64_t)f << lg) + pc * kV) = *reinterpret_cast<const uint4 *>(v);
     }
 }
 
 __global__ void __launch_bounds__(kCopyThreads)
     k_copy_rows(const NetDev *__restrict__ nets, int nnets, unsigned long long *launches) {
     count_launch(launches);
-    __shared__ uint4 stage[kCopyStageBytes / 16];
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t nth = (int64_t)gridDim.x * blockDim.x;
-    int64_t rows_total = 0, tiles = 0;
-    for (int n = 0; n < nnets; ++n) {
-        const NetDev &nd = nets[n];
-        if (nd.layout >= 2) tiles += (int64_t)((nd.st->copy_R + nd.layout - 1) / nd.layout) * copy_chunks(nd, gridDim.x);
-        else rows_total += nd.st->copy_R;
-    }
+    int64_t rows_total = 0;
+    for (int n = 0; n < nnets; ++n)
+        if (nets[n].layout < 2) rows_total += nets[n].st->copy_R;
     // row-major and MMA-tile nets: one warp per kept row, lanes over its
     // 16-byte pieces (8 features for 16-bit types, 4 for FP32)
     const int lane = threadIdx.x & 31;
@@ -594,23 +563,23 @@ __global__ void __launch_bounds__(kCopyThreads)
             *reinterpret_cast<uint4 *>(dst + act_index(nd.layout, N, q, f) * es) = v;
         }
     }
-    // row-tile nets: items of (destination tile, feature chunk)
+    // row-tile nets: one CTA per destination tile (copy_tile)
+    __shared__ int s_map[kCopyMaxTR];
+    int64_t tiles = 0;
+    for (int n = 0; n < nnets; ++n)
+        if (nets[n].layout >= 2) tiles += (nets[n].st->copy_R + nets[n].layout - 1) / nets[n].layout;
     for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         int64_t u = t;
-        int n = 0, nfc = 1;
+        int n = 0;
         for (; n < nnets; ++n) {
             const NetDev &nd = nets[n];
             if (nd.layout < 2) continue;
-            nfc = copy_chunks(nd, gridDim.x);
-            const int64_t cnt = (int64_t)((nd.st->copy_R + nd.layout - 1) / nd.layout) * nfc;
+            const int64_t cnt = (nd.st->copy_R + nd.layout - 1) / nd.layout;
             if (u < cnt) break;
             u -= cnt;
         }
-        const int per = ((nets[n].N + nfc - 1) / nfc + 7) / 8 * 8;  // features per chunk
-        const int tq = (int)(u / nfc), fb = min(nets[n].N, (int)(u % nfc) * per);
-        const int fe = min(nets[n].N, fb + per);
-        if (nets[n].prec == COSPDNN_PREC_FP32) copy_tile<uint32_t>(nets[n], tq, fb, fe, stage);
-        else copy_tile<uint16_t>(nets[n], tq, fb, fe, stage);
+        if (nets[n].prec == COSPDNN_PREC_FP32) copy_tile<float>(nets[n], (int)u, s_map);
+        else copy_tile<uint16_t>(nets[n], (int)u, s_map);
     }
 }
 
