@@ -44,7 +44,8 @@ namespace {
 constexpr size_t kCcPairBudget = 96 * 1024;
 constexpr size_t kCcTileBudget = 200 * 1024;
 constexpr int kCcMaxTR = 128;
-constexpr int kQB = 4;  // 16-byte entry groups per block
+constexpr int kQB = 4;   // 16-byte entry groups per block
+constexpr int kQBc = 2;  // the same for compact entry lists (16 entries per block, as 16-bit nets)
 
 // Entry blocks held in registers (the load of block s+ring-1 overlaps block
 // s): measured on one B200, two for 16-bit types (3% faster than three at
@@ -141,25 +142,39 @@ __device__ __forceinline__ void cc_entry(float *acc, uint32_t w, uint32_t addr) 
 // entries of a 16-bit net ((column << 16) | weight bits, 4 per group) or 8 of
 // an FP32 net ({column, weight bits}, 2 per group); column = the input's
 // LB-byte column in the tile (input * G).
-template <typename T, int LB>
-__device__ __forceinline__ void cc_block(float *acc, const uint4 *q, uint32_t sbase) {
+template <typename T, int LB, bool CMP>
+__device__ __forceinline__ void cc_block(float *acc, const uint4 *q, uint32_t sbase, uint32_t wconst) {
     constexpr int SH = LB == 16 ? 4 : 3;
+    if constexpr (CMP) {
+        // compact entries: eight 16-bit columns per group, one weight value
 #pragma unroll
-    for (int i = 0; i < kQB; ++i) {
-        if constexpr (sizeof(T) == 4) {
-            cc_entry<T, LB>(acc, q[i].y, sbase + (q[i].x << SH));
-            cc_entry<T, LB>(acc, q[i].w, sbase + (q[i].z << SH));
-        } else {
+        for (int i = 0; i < kQBc; ++i) {
             const uint32_t ent[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
 #pragma unroll
-            for (int e = 0; e < 4; ++e) cc_entry<T, LB>(acc, ent[e], sbase + ((ent[e] >> 16) << SH));
+            for (int e = 0; e < 4; ++e) {
+                cc_entry<T, LB>(acc, wconst, sbase + ((ent[e] & 0xFFFFu) << SH));
+                cc_entry<T, LB>(acc, wconst, sbase + ((ent[e] >> 16) << SH));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kQB; ++i) {
+            if constexpr (sizeof(T) == 4) {
+                cc_entry<T, LB>(acc, q[i].y, sbase + (q[i].x << SH));
+                cc_entry<T, LB>(acc, q[i].w, sbase + (q[i].z << SH));
+            } else {
+                const uint32_t ent[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) cc_entry<T, LB>(acc, ent[e], sbase + ((ent[e] >> 16) << SH));
+            }
         }
     }
 }
 
+template <int QB>
 __device__ __forceinline__ void cc_load(uint4 *q, const uint4 *__restrict__ W, int N, int j, int b) {
 #pragma unroll
-    for (int i = 0; i < kQB; ++i) q[i] = __ldg(W + (int64_t)(b * kQB + i) * N + j);
+    for (int i = 0; i < QB; ++i) q[i] = __ldg(W + (int64_t)(b * QB + i) * N + j);
 }
 
 // Bytes of a feature column a lane owns: 16 when the tile's column has 16 or
@@ -168,9 +183,10 @@ __host__ __device__ __forceinline__ int cc_lane_bytes_of(int prec, int TR) {
     return TR * (prec == COSPDNN_PREC_FP32 ? 4 : 2) >= 16 ? 16 : 8;
 }
 
-__device__ __forceinline__ bool cc_net(const NetDev &nd, int prec, int lb) {
+__device__ __forceinline__ bool cc_net(const NetDev &nd, int prec, int lb, bool cmp) {
     return nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 2 && nd.prec == prec && !nd.st->done &&
-           cc_lane_bytes_of(nd.prec, nd.layout) == lb && !(nd.st->layer == 0 && nd.st->l0_bits);
+           cc_lane_bytes_of(nd.prec, nd.layout) == lb && (nd.cc_compact != 0) == cmp &&
+           !(nd.st->layer == 0 && nd.st->l0_bits);
 }
 
 // Output slices per tile: the split (1, 2, 4, ... up to one CTA round of
@@ -199,11 +215,11 @@ struct CcItem {
     int net, tile, slice, slices;
 };
 
-__device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int prec, int lb, int grid, int warps,
+__device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int prec, int lb, bool cmp, int grid, int warps,
                                           int64_t u, CcItem &it) {
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (!cc_net(nd, prec, lb)) continue;
+        if (!cc_net(nd, prec, lb, cmp)) continue;
         const int S = cc_slices(nd, grid, warps);
         const int64_t cnt = (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * S;
         if (u < cnt) {
@@ -263,12 +279,13 @@ __device__ __forceinline__ void cc_store(float *acc, float *zmax, float *zdist, 
     else *reinterpret_cast<uint2 *>(dst) = *reinterpret_cast<const uint2 *>(ov);
 }
 
-template <typename T, int NT, int LB>
+template <typename T, int NT, int LB, bool CMP>
 __global__ void __launch_bounds__(NT, 512 / NT)
     k_layer_cc(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
     count_launch(launches);
     constexpr int ES = (int)sizeof(T), V = LB / ES, kWarps = NT / 32;
-    constexpr int EB = kQB * cc_epv<T>();  // entries per block
+    constexpr int QB = CMP ? kQBc : kQB;                 // 16-byte groups per block
+    constexpr int EB = QB * (CMP ? 8 : cc_epv<T>());      // entries per block
     constexpr int kRing = cc_ring<T>();
     extern __shared__ uint4 cc_smem[];
     __shared__ uint32_t s_zmax[kCcMaxTR], s_zdist[kCcMaxTR];
@@ -277,12 +294,12 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     int64_t total = 0;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (!cc_net(nd, prec, LB)) continue;
+        if (!cc_net(nd, prec, LB, CMP)) continue;
         total += (int64_t)((nd.st->R + nd.layout - 1) / nd.layout) * cc_slices(nd, grid, kWarps);
     }
     for (int64_t item = blockIdx.x; item < total; item += grid) {
         CcItem it;
-        cc_locate(nets, nnets, prec, LB, grid, kWarps, item, it);
+        cc_locate(nets, nnets, prec, LB, CMP, grid, kWarps, item, it);
         const NetDev &nd = nets[it.net];
         const int N = nd.N, TR = nd.layout, l = nd.st->layer, R = nd.st->R, par = l & 1, ib = nd.st->in_buf;
         const LayerDev &lw = nd.layers[l];
@@ -306,6 +323,9 @@ __global__ void __launch_bounds__(NT, 512 / NT)
                 for (int k = 0; k < 8; ++k) cc_smem[i + k * NT] = v[k];
             }
             for (; i < nvec; i += NT) cc_smem[i] = __ldg(src + i);
+            // the zero columns after the N inputs (read by padding entries)
+            for (int z = threadIdx.x; z < kCcZeroCols * TR * ES / 16; z += NT)
+                cc_smem[nvec + z] = make_uint4(0u, 0u, 0u, 0u);
             for (int r = threadIdx.x; r < TR; r += NT) {
                 s_zmax[r] = 0u;
                 s_zdist[r] = 0x7F800000u;  // +inf
@@ -314,7 +334,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
         if (threadIdx.x == 0 && item + grid < total) {
             // the next tile of this CTA into L2 while this one is computed
             CcItem nx;
-            if (cc_locate(nets, nnets, prec, LB, grid, kWarps, item + grid, nx) &&
+            if (cc_locate(nets, nnets, prec, LB, CMP, grid, kWarps, item + grid, nx) &&
                 (nx.net != it.net || nx.tile != it.tile)) {
                 const NetDev &nn = nets[nx.net];
                 const T *nin = (const T *)(nn.st->layer == 0 ? nn.y0 : nn.act[nn.st->in_buf]);
@@ -347,9 +367,10 @@ __global__ void __launch_bounds__(NT, 512 / NT)
             zdist[v] = INFINITY;
         }
         int jl = j0, bl = 0, jc = j0, bc = 0;
-        uint4 q[kRing][kQB];
+        const uint32_t wconst = lw.cc_wconst;
+        uint4 q[kRing][QB];
         auto next_load = [&](uint4 *q) {
-            cc_load(q, W, N, jl, bl);
+            cc_load<QB>(q, W, N, jl, bl);
             if (++bl == nb) {
                 bl = 0;
                 jl += step;
@@ -370,7 +391,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
             for (int r = 0; r < kRing; ++r) {  // buffer indices are compile-time
                 if (s + r >= nsteps) break;
                 if (s + r + kRing - 1 < nsteps) next_load(q[(r + kRing - 1) % kRing]);
-                cc_block<T, LB>(acc, q[r], sbase);
+                cc_block<T, LB, CMP>(acc, q[r], sbase, wconst);
                 finish_step();
             }
         }
@@ -404,6 +425,13 @@ __global__ void __launch_bounds__(NT, 512 / NT)
             }
         }
     }
+}
+
+// A weight as the compute type holds it.
+float to_compute_weight(float w, int prec) {
+    if (prec == COSPDNN_PREC_FP16) return __half2float(__float2half_rn(w));
+    if (prec == COSPDNN_PREC_BF16) return __bfloat162float(__float2bfloat16_rn(w));
+    return w;
 }
 
 template <typename T>
@@ -494,12 +522,22 @@ int cc_tile_rows(int N, int prec) {
     for (int lb : {16, 8})
         for (size_t budget : {kCcPairBudget, kCcTileBudget})
             for (int TR = kCcMaxTR; TR >= 1; TR >>= 1)
-                if (TR * es >= lb && (size_t)N * TR * es <= budget) return TR;
+                if (TR * es >= lb && cc_tile_bytes(N, prec, TR) <= budget) return TR;
     return 0;
 }
 
+bool cc_single_weight(const std::vector<int32_t> &colptr, const std::vector<float> &vals, int N, int prec) {
+    const int64_t nnz = colptr[N];
+    if (nnz == 0) return false;
+    const float w0 = to_compute_weight(vals[0], prec);
+    if (w0 == 0.0f) return false;
+    for (int64_t p = 1; p < nnz; ++p)
+        if (to_compute_weight(vals[p], prec) != w0) return false;
+    return true;
+}
+
 int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx,
-                     const std::vector<float> &vals, int N, int prec, int TR, LayerDev &ld,
+                     const std::vector<float> &vals, int N, int prec, int TR, bool compact, LayerDev &ld,
                      std::vector<void *> &owned) {
     const int es = prec == COSPDNN_PREC_FP32 ? 4 : 2;
     // A lane owns an LB-byte piece of a feature column; shared loads are served
@@ -511,7 +549,8 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
     const int B = colw >= phase ? 1 : phase / colw;        // outputs per wavefront
     const int P = B;                                       // residues that must differ
     CSP_CHECK(colw >= 1 && N % B == 0, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: bad tile");
-    CSP_CHECK((size_t)N * colw <= 65536, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: tile too large");
+    CSP_CHECK((size_t)(N + kCcZeroCols) * colw <= 65536, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: tile too large");
+    CSP_CHECK(P <= kCcZeroCols, COSPDNN_ERR_UNSUPPORTED, "cc_build_entries: too many residues");
     // groups of outputs whose entries must have distinct residues mod P at
     // every step: the B outputs of a wavefront
     std::vector<std::vector<int>> groups;
@@ -549,7 +588,7 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
         }
     }
     const int Kc = (Kmax + 15) / 16 * 16;
-    const int epv = es == 4 ? 2 : 4;  // entries per 16-byte group
+    const int epv = compact ? 8 : (es == 4 ? 2 : 4);  // entries per 16-byte group
     const size_t ngroups = (size_t)Kc / epv;
     std::vector<uint32_t> packed(ngroups * N * 4, 0u);
     for (const auto &grp : groups) {
@@ -571,13 +610,18 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
                         while (used & (1u << r)) ++r;  // fewer than P residues are taken
                         used |= 1u << r;
                     }
-                    idx = r;  // residue r (N >= P)
+                    // residue r: input r with weight 0 (N >= P), or for a
+                    // compact list the zero column of residue r after the N inputs
+                    idx = compact ? N + ((r - N % P) % P + P) % P : r;
                     w = 0.0f;
                 }
                 const size_t g = (size_t)(t / epv), slot = (size_t)(t % epv);
                 uint32_t *dst = &packed[(g * N + j) * 4];
                 const uint32_t col = (uint32_t)idx * colw;  // first LB-byte column of the input
-                if (es == 4) {
+                if (compact) {
+                    // entry 2k in the low half of word k, entry 2k+1 in its high half
+                    dst[slot / 2] |= col << (16 * (slot % 2));
+                } else if (es == 4) {
                     dst[2 * slot] = col;
                     uint32_t wb;
                     std::memcpy(&wb, &w, 4);
@@ -596,20 +640,28 @@ int cc_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32
     CSP_CUDA(cudaMemcpy(d, packed.data(), packed.size() * 4, cudaMemcpyHostToDevice));
     ld.cc_w = (const uint4 *)d;
     ld.cc_k = Kc;
+    ld.cc_wconst = 0u;
+    if (compact) {
+        const float w = to_compute_weight(vals[0], prec);
+        if (es == 4) std::memcpy(&ld.cc_wconst, &w, 4);
+        else ld.cc_wconst = prec == COSPDNN_PREC_FP16 ? weight_bits<__half>(w) : weight_bits<__nv_bfloat16>(w);
+    }
     return COSPDNN_OK;
 }
 
-int cc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, int lane_bytes, unsigned long long *launches,
-                  int sms, size_t max_tile_bytes) {
+int cc_layer_spec(KSpec &k, NetDev *nets, int nnets, int prec, int lane_bytes, bool compact,
+                  unsigned long long *launches, int sms, size_t max_tile_bytes) {
     using F = void (*)(const NetDev *, int, int, unsigned long long *);
-    static const F fns[3][2][2] = {
-        {{k_layer_cc<float, 512, 16>, k_layer_cc<float, 512, 8>}, {k_layer_cc<float, 256, 16>, k_layer_cc<float, 256, 8>}},
-        {{k_layer_cc<__half, 512, 16>, k_layer_cc<__half, 512, 8>},
-         {k_layer_cc<__half, 256, 16>, k_layer_cc<__half, 256, 8>}},
-        {{k_layer_cc<__nv_bfloat16, 512, 16>, k_layer_cc<__nv_bfloat16, 512, 8>},
-         {k_layer_cc<__nv_bfloat16, 256, 16>, k_layer_cc<__nv_bfloat16, 256, 8>}}};
+#define CSP_CC(T, NT)                                                                     \
+    {{k_layer_cc<T, NT, 16, false>, k_layer_cc<T, NT, 16, true>},                         \
+     {k_layer_cc<T, NT, 8, false>, k_layer_cc<T, NT, 8, true>}}
+    // [precision][one CTA of 512 / two of 256 per SM][lane bytes 16 / 8][compact entries]
+    static const F fns[3][2][2][2] = {{CSP_CC(float, 512), CSP_CC(float, 256)},
+                                      {CSP_CC(__half, 512), CSP_CC(__half, 256)},
+                                      {CSP_CC(__nv_bfloat16, 512), CSP_CC(__nv_bfloat16, 256)}};
+#undef CSP_CC
     const bool pair = max_tile_bytes <= kCcPairBudget;
-    k.fn = (void *)fns[prec][pair ? 1 : 0][lane_bytes == 16 ? 0 : 1];
+    k.fn = (void *)fns[prec][pair ? 1 : 0][lane_bytes == 16 ? 0 : 1][compact ? 1 : 0];
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_tile_bytes));
     k.grid = dim3(pair ? 2 * sms : sms);
     k.block = dim3(pair ? 256 : 512);

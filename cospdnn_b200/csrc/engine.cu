@@ -443,7 +443,8 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
         int rc = tc_build_blocks(h.colptr, h.rowidx, h.vals, N, net.d.precision, ld, e->owned);
         if (rc) return rc;
     } else if (const int TR = cc_tile_rows(N, net.d.precision)) {
-        int rc = cc_build_entries(h.colptr, h.rowidx, h.vals, N, net.d.precision, TR, ld, e->owned);
+        int rc = cc_build_entries(h.colptr, h.rowidx, h.vals, N, net.d.precision, TR, net.dev.cc_compact != 0, ld,
+                                  e->owned);
         if (rc) return rc;
     }
     return COSPDNN_OK;
@@ -452,7 +453,7 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
 // Precisions of the nets on each layer kernel.
 struct KernelSets {
     std::vector<int> plain, tc;
-    // row-tile kernel: (precision, lane bytes) -> largest row tile of those nets
+    // row-tile kernel: (precision, lane bytes | compact entries << 8) -> largest row tile of those nets
     std::vector<std::pair<std::pair<int, int>, size_t>> cc;
 };
 
@@ -482,7 +483,9 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
     }
     for (const auto &cc : ks.cc) {
         KSpec k;
-        int rc = cc_layer_spec(k, nets, nn, cc.first.first, cc.first.second, launches, sms, cc.second);
+        // key: precision, lane bytes | compact entries << 8
+        int rc = cc_layer_spec(k, nets, nn, cc.first.first, cc.first.second & 0xff, (cc.first.second >> 8) != 0,
+                               launches, sms, cc.second);
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
@@ -718,7 +721,14 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         // kernel) or row-major (CUDA-core gather kernel, rows too wide for a tile)
         n.dev.layout = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? 1 : cc_tile_rows(n.d.neuron, n.d.precision);
         if (n.dev.layout >= 2) {
-            const std::pair<int, int> key(n.d.precision, cc_lane_bytes(n.d.precision, n.dev.layout));
+            // compact entry lists when every layer has one weight value (the
+            // Graph Challenge networks): 2 bytes per entry instead of 4 or 8
+            bool compact = true;
+            for (int l = 0; l < n.d.layers && compact; ++l)
+                compact = cc_single_weight(n.layers[l].colptr, n.layers[l].vals, n.d.neuron, n.d.precision);
+            n.dev.cc_compact = compact ? 1 : 0;
+            const std::pair<int, int> key(n.d.precision,
+                                          cc_lane_bytes(n.d.precision, n.dev.layout) | (n.dev.cc_compact << 8));
             const size_t tb = cc_tile_bytes(n.d.neuron, n.d.precision, n.dev.layout);
             auto it = std::find_if(ks.cc.begin(), ks.cc.end(), [&](const auto &x) { return x.first == key; });
             if (it == ks.cc.end()) ks.cc.push_back({key, tb});

@@ -59,12 +59,16 @@ struct LayerDev {
     int tc_nchunks;
     int max_blocks;  // max 16x16 blocks in one output block column (error bound)
     // CUDA-core tile kernel (k_layer_cc): per output j, cc_k entries (input
-    // index, weight in the compute type) in a build-time order, zero-weight
-    // padding included; 16-byte groups of entries stored group-major,
-    // [group][j] (16-bit nets: 4 entries of idx | w << 16; FP32 nets:
-    // 2 entries of {idx, w bits}), so consecutive outputs are adjacent.
+    // column, weight in the compute type) in a build-time order, padding
+    // included; 16-byte groups of entries stored group-major, [group][j]
+    // (16-bit nets: 4 entries of col << 16 | w; FP32 nets: 2 entries of
+    // {col, w bits}; compact nets: 8 entries of a 16-bit col, the weight being
+    // cc_wconst and padding pointing at a zero column), so consecutive
+    // outputs are adjacent.
     const uint4 *cc_w;
     int cc_k;
+    uint32_t cc_wconst;  // compact entry lists (NetDev::cc_compact): the layer's one weight value, its
+                         // bits in the compute type (16-bit types in the low half)
     float S;         // max_j sum_i |W_ij|
     float dW;        // max_j sum_i |W'_ij - W_ij|, W' = weights in the compute type
 };
@@ -90,6 +94,7 @@ struct NetDev {
     const float *err0;       // [rows] bound on |y0(compute) - y0(exact)|
     const float *mx0;        // [rows] max |y0|
     int layout;              // activation layout: 0 row-major, 1 MMA tiles, >= 2 row tiles (see act_index)
+    int cc_compact;          // row-tile nets: 16-bit entries (input column only), every layer one weight value
     void *act[2];            // ping-pong activations, rows padded to a multiple of 128
     int32_t *cmap;           // [rows] compaction map: new row q <- output row cmap[q]
     int32_t *orig[2];        // list: original row id
