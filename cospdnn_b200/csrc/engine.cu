@@ -1259,9 +1259,11 @@ namespace {
 // layer_ms the layer kernels of iteration i are timed into layer_ms[i].
 // Stops after max_iters iterations, when every network is done, or (stop_net
 // >= 0) once network stop_net has computed layer stop_layer or finished.
+// With start false the loop resumes a stopped pass at iteration it0 (no new
+// inputs, no reset of the states).
 int eager_run(cospdnn_engine *e, cudaStream_t s, int max_iters, float *layer_ms, int *iters, int stop_net,
-              int stop_layer) {
-    int rc = take_inputs(e, s);
+              int stop_layer, bool start = true, int it0 = 0) {
+    int rc = start ? take_inputs(e, s) : COSPDNN_OK;
     if (rc) return rc;
     cudaEvent_t a, b;
     CSP_CUDA(cudaEventCreate(&a));
@@ -1272,8 +1274,8 @@ int eager_run(cospdnn_engine *e, cudaStream_t s, int max_iters, float *layer_ms,
             return cuda_fail(err, "eager run: event");
         }
     }
-    rc = launch(e->k0, s);
-    int it = 0;
+    if (start) rc = launch(e->k0, s);
+    int it = it0;
     std::vector<NetState> st(e->nets.size());
     while (!rc && it < max_iters) {
         bool live = false;
@@ -1338,12 +1340,17 @@ extern "C" int cospdnn_engine_layer_values(cospdnn_engine *e, int net, int layer
     DeviceGuard g(e->device);
     cudaStream_t s = (cudaStream_t)stream;
     *count = 0;
-    int rc = eager_run(e, s, e->max_layers + 1, nullptr, nullptr, net, layer);
+    int it = 0;
+    int rc = eager_run(e, s, e->max_layers + 1, nullptr, &it, net, layer);
     if (rc) return rc;
     NetState st;
     CSP_CUDA(cudaMemcpyAsync(&st, e->nets[net].dev.st, sizeof(st), cudaMemcpyDeviceToHost, s));
     CSP_CUDA(cudaStreamSynchronize(s));
     CSP_CHECK(st.err == 0, COSPDNN_ERR_DEVICE, "layer_values: device-side check failed");
-    if (st.layer != layer + 1) return COSPDNN_OK;  // every row was pruned before `layer`
-    return copy_current_rows(e, net, out, ids, bounds, max_rows, count, s);
+    // rows of `layer` (none when every row was pruned before it)
+    if (st.layer == layer + 1) rc = copy_current_rows(e, net, out, ids, bounds, max_rows, count, s);
+    if (rc) return rc;
+    // the pass runs on to the end, so that every network's result is again
+    // that of a complete run
+    return eager_run(e, s, e->max_layers + 1, nullptr, nullptr, -1, 0, false, it);
 }

@@ -231,7 +231,9 @@ int cospdnn_engine_final_values(cospdnn_engine *e, int net, float *out, int64_t 
  * NULL; the bound behind the exact keep/prune decisions), the row count into
  * *count (0 when every row was pruned at or before `layer`).  Replaces the reference's
  * -DPRINT_RESULT dump of C (src/cospdnn.cu:311-320) for any layer; for checks
- * against an FP64 recurrence.  Synchronizes `stream`. */
+ * against an FP64 recurrence.  The eager pass then runs on to the end, so
+ * afterwards every network's cospdnn_engine_result and final values are
+ * those of a complete run on the current inputs.  Synchronizes `stream`. */
 int cospdnn_engine_layer_values(cospdnn_engine *e, int net, int layer, float *out, int32_t *ids,
                                 float *bounds, int64_t max_rows, int64_t *count, void *stream);
 /* Largest of the surviving rows' proven bounds on |final value - FP64

@@ -178,3 +178,22 @@ def test_layer_values_and_final_values_bounds(cs, oracle):
     # a layer before the last: rows kept after it, and every value within bound
     check_values(oracle, eng, nid, csc, y0, b, 2, max_rows=700)
     eng.close()
+
+
+def test_layer_values_leaves_every_network_finished(cs):
+    """layer_values of one network stops the eager pass at that layer to copy
+    its rows, then runs the pass on to the end: afterwards every network's
+    result equals the graph run's (the parity check of a multi-network
+    configuration reads results after values)."""
+    nets = [make_net(1024, 8, 900, seed=SEED + 11, dlo=0.25, dhi=0.45),
+            make_net(4096, 10, 700, seed=SEED + 12, dlo=0.2, dhi=0.4)]
+    eng, ids = build(cs, nets, cs.PREC_FP16)
+    eng.run()
+    want = [eng.result(nid) for nid in ids]
+    vals, rid = eng.layer_values(ids[0], 1)
+    assert len(rid) > 0
+    for nid, w in zip(ids, want):
+        r = eng.result(nid)
+        np.testing.assert_array_equal(r["alive"], w["alive"])
+        np.testing.assert_array_equal(r["categories"], w["categories"])
+    eng.close()
