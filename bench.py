@@ -101,6 +101,13 @@ PARITY_ROWS = {1024: 60000, 4096: 60000, 16384: 16384, 65536: 2048}
 DY_ROWS = 2048  # rows per checked layer compared value by value
 
 
+def is_split(info, prec):
+    """Feature-split nets: CUDA cores with 2-row tiles of a 16-bit type (the
+    one-CTA row-tile kernel takes 16-bit tiles of 4 rows or more)."""
+    import cospdnn_b200 as cs
+    return info["kernel"] == cs.KERNEL_CUDA_CORE and info["row_tile"] == 2 and prec != "fp32"
+
+
 def layer_kernel_name(info, n, prec):
     """Name of the kernel that computes layers >= 1 of a net (engine's choice)."""
     import cospdnn_b200 as cs
@@ -110,6 +117,8 @@ def layer_kernel_name(info, n, prec):
     tr = info["row_tile"]
     if tr == 0:
         return f"k_layer_plain<{TNAME[prec]}>"
+    if is_split(info, prec):
+        return f"k_layer_cs<{TNAME[prec]}>"
     nt = 256 if n * tr * es <= 96 * 1024 else 512
     lb = 16 if tr * es >= 16 else 8
     return f"k_layer_cc<{TNAME[prec]}, {nt}, {lb}>"
@@ -119,7 +128,8 @@ def layer0_kernel_name(info, prec):
     import cospdnn_b200 as cs
     if not info["layer0_counted"]:
         return None
-    return f"k_layer0_bits16<{TNAME[prec]}>" if info["kernel"] == cs.KERNEL_TCGEN05 else f"k_layer0_bits<{TNAME[prec]}>"
+    sixteen = info["kernel"] == cs.KERNEL_TCGEN05 or is_split(info, prec)
+    return f"k_layer0_bits16<{TNAME[prec]}>" if sixteen else f"k_layer0_bits<{TNAME[prec]}>"
 
 
 def weight_bytes(info, n, prec):

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcospdnn_b200.so")
-SOURCES = ["layer_ref.cu", "engine.cu", "tc_layer.cu", "cc_layer.cu", "bits_layer.cu", "synth.cu"]
+SOURCES = ["layer_ref.cu", "engine.cu", "tc_layer.cu", "cc_layer.cu", "cs_layer.cu", "bits_layer.cu", "synth.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--expt-relaxed-constexpr", "-diag-suppress", "177"]

@@ -227,12 +227,13 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
 // (16 bits per feature) fit in shared memory up to 65536 features; a lane
 // packs two entries' 16-bit words into one 32-bit word (the even entry in
 // the low half), counts them as above and adds the two halves' counts; each
-// output value is stored into its MMA operand tile (act_index layout 1).
+// output value is stored into its MMA operand tile (act_index layout 1), or
+// (feature-split nets) into its 2-row tile word (layout 2).
 constexpr int kBits16Threads = 512;
 constexpr int kBits16Warps = kBits16Threads / 32;
 
 __device__ __forceinline__ bool l0_net16(const NetDev &nd, int prec) {
-    return nd.l0_k > 0 && nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.layout == 1 && nd.prec == prec &&
+    return nd.l0_k > 0 && ((nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.layout == 1) || nd.cc_split) && nd.prec == prec &&
            !nd.st->done && nd.st->layer == 0 && nd.y0bits != nullptr && *nd.y0nonbin == 0;
 }
 
@@ -300,6 +301,7 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                 const float w = nd.l0_w[j];
                 uint32_t c[8];
                 counts8(p, c);
+                T ov[16];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const uint32_t s2 = c[k] + (c[k] >> 16);  // even + odd entries' counts (each <= 32)
@@ -315,8 +317,20 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                         // the tcgen05 epilogue's error of an output near the clamp range
                         if (z > -ezr[r] && z < 32.0f + ezr[r])
                             ems[r] = fmaxf(ems[r], __fadd_ru(ezr[r], fabsf(act_traits<T>::to_f(o) - cz)));
-                        out[act_index(1, N, (int64_t)u * 16 + r, j)] = o;
+                        ov[r] = o;
                     }
+                }
+                if (nd.layout == 1) {
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) out[act_index(1, N, (int64_t)u * 16 + r, j)] = ov[r];
+                } else {
+                    // 2-row tiles (feature-split nets): one 4-byte word per row pair,
+                    // consecutive outputs adjacent
+#pragma unroll
+                    for (int r = 0; r < 16; r += 2)
+                        *reinterpret_cast<uint32_t *>(out + act_index(2, N, (int64_t)u * 16 + r, j)) =
+                            (uint32_t)*reinterpret_cast<const uint16_t *>(&ov[r]) |
+                            ((uint32_t)*reinterpret_cast<const uint16_t *>(&ov[r + 1]) << 16);
                 }
             }
 #pragma unroll

@@ -184,7 +184,7 @@ __host__ __device__ __forceinline__ int cc_lane_bytes_of(int prec, int TR) {
 }
 
 __device__ __forceinline__ bool cc_net(const NetDev &nd, int prec, int lb, bool cmp) {
-    return nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 2 && nd.prec == prec && !nd.st->done &&
+    return nd.kernel == COSPDNN_KERNEL_CUDA_CORE && nd.layout >= 2 && !nd.cc_split && nd.prec == prec && !nd.st->done &&
            cc_lane_bytes_of(nd.prec, nd.layout) == lb && (nd.cc_compact != 0) == cmp &&
            !(nd.st->layer == 0 && nd.st->l0_bits);
 }
@@ -232,33 +232,6 @@ __device__ __forceinline__ bool cc_locate(const NetDev *nets, int nnets, int pre
         u -= cnt;
     }
     return false;
-}
-
-// Bound on |stored - clamped| for a value c in [0, 32] stored in the compute
-// type: half an ulp, at most 2^-11 c + 2^-25 (FP16; 2^-25 covers the
-// subnormal range) or 2^-8 c + 2^-126 (BF16, more than its subnormal half
-// spacing); 0 for FP32.
-template <typename T>
-__device__ __forceinline__ float store_error(float c) {
-    if constexpr (sizeof(T) == 4) return 0.0f;
-    else if constexpr (std::is_same<T, __half>::value) return __fmaf_ru(c, 4.8828125e-04f, 2.98023224e-08f);
-    else return __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
-}
-
-// Row statistics from the row's max pre-activation zm, its min |z - 16|
-// over the outputs (zd) and its error bound ez:
-//   max output  = the stored value of clamp(zm) (rounding is monotone, so
-//                 this is the max of the stored outputs);
-//   output error: outputs with z <= -ez are 0 in both recurrences and those
-//                 with z >= 32 + ez are 32 in both; the others, those with
-//                 |z - 16| < 16 + ez (there are some iff zd < 16 + ez), are
-//                 within ez of the exact clamp plus their storage rounding,
-//                 at most clamp(zm): bound ez + store_error(clamp(zm)), else 0.
-template <typename T>
-__device__ __forceinline__ void row_stats(float zm, float zd, float ez, float &emax, float &ymax) {
-    const float c = clamp32(zm);
-    ymax = act_traits<T>::to_f(act_traits<T>::from_f(c));
-    emax = zd < 16.0f + ez ? __fadd_ru(ez, store_error<T>(c)) : 0.0f;
 }
 
 // Bias, clamp, store of V accumulators as one LB-byte piece; per row the max

@@ -9,6 +9,7 @@
 
 #include "bits_layer.cuh"
 #include "cc_layer.cuh"
+#include "cs_layer.cuh"
 #include "engine_kernels.cuh"
 #include "tc_layer.cuh"
 
@@ -399,12 +400,13 @@ double blocks_per_column(const HostLayer &h, int N) {
 // 60000 rows, FP16): one layer takes 0.86 ms on CUDA cores for any pattern,
 // 2.13 ms on tcgen05 at 29 blocks per block column (fill 1/16, XOR masks) and
 // 0.39 ms at 2 (fill 1); the lines cross near 9.5 blocks, fill 0.21.  So
-// tcgen05 when its blocks are at least a quarter full or when the row tile
-// of the CUDA-core kernel does not fit; FP32 always on CUDA cores.
+// tcgen05 when its blocks are at least a quarter full or when neither the
+// row tile of the CUDA-core kernel nor half of a 2-row tile (feature-split
+// kernel) fits; FP32 always on CUDA cores.
 int auto_kernel(const Net &n) {
     const int N = n.d.neuron, prec = n.d.precision;
     if (prec == COSPDNN_PREC_FP32 || !tc_supported(N)) return COSPDNN_KERNEL_CUDA_CORE;
-    if (cc_tile_rows(N, prec) == 0) return COSPDNN_KERNEL_TCGEN05;
+    if (cc_tile_rows(N, prec) == 0 && !cs_supported(N, prec)) return COSPDNN_KERNEL_TCGEN05;
     return block_fill(n) >= 0.25 ? COSPDNN_KERNEL_TCGEN05 : COSPDNN_KERNEL_CUDA_CORE;
 }
 
@@ -442,6 +444,10 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
     if (net.dev.kernel == COSPDNN_KERNEL_TCGEN05) {
         int rc = tc_build_blocks(h.colptr, h.rowidx, h.vals, N, net.d.precision, ld, e->owned);
         if (rc) return rc;
+    } else if (net.dev.cc_split) {
+        int rc = cs_build_entries(h.colptr, h.rowidx, h.vals, N, net.d.precision, net.dev.cc_compact != 0, ld,
+                                  e->owned);
+        if (rc) return rc;
     } else if (const int TR = cc_tile_rows(N, net.d.precision)) {
         int rc = cc_build_entries(h.colptr, h.rowidx, h.vals, N, net.d.precision, TR, net.dev.cc_compact != 0, ld,
                                   e->owned);
@@ -455,6 +461,8 @@ struct KernelSets {
     std::vector<int> plain, tc;
     // row-tile kernel: (precision, lane bytes | compact entries << 8) -> largest row tile of those nets
     std::vector<std::pair<std::pair<int, int>, size_t>> cc;
+    // feature-split kernel: (precision, compact entries) -> widest of those nets
+    std::vector<std::pair<std::pair<int, int>, int>> cs;
 };
 
 int make_specs(cospdnn_engine *e, const KernelSets &ks) {
@@ -493,7 +501,7 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         for (int prec = 0; prec < 3; ++prec) {
             int max_n = 0;
             for (const Net &n : e->nets)
-                if (n.dev.l0_k > 0 && n.d.precision == prec && (n.dev.layout == 1) == (mma == 1))
+                if (n.dev.l0_k > 0 && n.d.precision == prec && (n.dev.layout == 1 || n.dev.cc_split) == (mma == 1))
                     max_n = std::max(max_n, n.d.neuron);
             if (!max_n) continue;
             KSpec k;
@@ -501,6 +509,13 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
             if (rc) return rc;
             e->l0_specs.push_back(std::move(k));
         }
+    for (const auto &c : ks.cs) {
+        KSpec k;
+        int rc = cs_layer_spec(k, nets, nn, c.first.first, c.first.second != 0, launches, e->abort_flag, e->limits, sms,
+                               c.second);
+        if (rc) return rc;
+        e->layer_specs.push_back(std::move(k));
+    }
     for (int prec : ks.tc) {
         KSpec k;
         int rc = tc_layer_spec(k, nets, nn, prec, launches, e->abort_flag, e->limits, sms);
@@ -720,6 +735,12 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         // activation layout: MMA tiles (tcgen05), row tiles (CUDA-core tile
         // kernel) or row-major (CUDA-core gather kernel, rows too wide for a tile)
         n.dev.layout = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 ? 1 : cc_tile_rows(n.d.neuron, n.d.precision);
+        n.dev.cc_split = 0;
+        if (n.dev.kernel == COSPDNN_KERNEL_CUDA_CORE && n.dev.layout == 0 && cs_supported(n.d.neuron, n.d.precision)) {
+            // 2-row tiles split by feature over the two CTAs of a cluster
+            n.dev.layout = 2;
+            n.dev.cc_split = 1;
+        }
         if (n.dev.layout >= 2) {
             // compact entry lists when every layer has one weight value (the
             // Graph Challenge networks): 2 bytes per entry instead of 4 or 8
@@ -727,6 +748,13 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
             for (int l = 0; l < n.d.layers && compact; ++l)
                 compact = cc_single_weight(n.layers[l].colptr, n.layers[l].vals, n.d.neuron, n.d.precision);
             n.dev.cc_compact = compact ? 1 : 0;
+            if (n.dev.cc_split) {
+                const std::pair<int, int> key(n.d.precision, n.dev.cc_compact);
+                auto it = std::find_if(ks.cs.begin(), ks.cs.end(), [&](const auto &x) { return x.first == key; });
+                if (it == ks.cs.end()) ks.cs.push_back({key, n.d.neuron});
+                else it->second = std::max(it->second, n.d.neuron);
+                continue;
+            }
             const std::pair<int, int> key(n.d.precision,
                                           cc_lane_bytes(n.d.precision, n.dev.layout) | (n.dev.cc_compact << 8));
             const size_t tb = cc_tile_bytes(n.d.neuron, n.d.precision, n.dev.layout);
@@ -749,10 +777,13 @@ extern "C" int cospdnn_engine_build(cospdnn_engine *e) {
         const bool l0_mma = n.dev.kernel == COSPDNN_KERNEL_TCGEN05 && n.dev.layout == 1 &&
                             n.d.precision != COSPDNN_PREC_FP32 && n.d.layers > 0 &&
                             blocks_per_column(n.layers[0], N) >= 6.0;
-        if ((l0_rows || l0_mma) && n.d.layers > 0) {
+        // feature-split nets: the 16-row counting kernel (a 32-row unit of
+        // 65536 features does not fit shared memory), stores into 2-row tiles
+        const bool l0_split = n.dev.cc_split != 0;
+        if ((l0_rows || l0_mma || l0_split) && n.d.layers > 0) {
             const HostLayer &h0 = n.layers[0];
-            int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, n.dev.layout, n.d.bias, n.dev,
-                              e->owned);
+            int rc = l0_build(h0.colptr, h0.rowidx, h0.vals, N, n.d.precision, l0_split ? 1 : n.dev.layout, n.d.bias,
+                              n.dev, e->owned);
             if (rc) return rc;
             if (n.dev.l0_k > 0) {
                 for (int b = 0; b < 2; ++b) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -69,6 +70,18 @@ struct LayerDev {
     int cc_k;
     uint32_t cc_wconst;  // compact entry lists (NetDev::cc_compact): the layer's one weight value, its
                          // bits in the compute type (16-bit types in the low half)
+    // Feature-split tile kernel (k_layer_cs, NetDev::cc_split): the inputs
+    // are split in two halves by bit cs_bit of the feature index (CTA h of a
+    // cluster holds the features whose bit is h, in ascending order).  Per
+    // half h, round k, warp w, column t < cs_cnt, slot s and lane, one 16-byte
+    // entry group at cs_w[((((h * rounds + k) * 16 + w) * cs_cnt + t) * 4 + s)
+    // * 32 + lane] for output lane of group s * rounds * 16 + 16 k + w (groups
+    // of 32 outputs, padded to a multiple of 64): compact lists four byte
+    // offsets of the inputs' 2-row words in the CTA's tile, else two
+    // {offset, weight bits} pairs.
+    const uint4 *cs_w;
+    int cs_cnt;
+    int cs_bit;
     float S;         // max_j sum_i |W_ij|
     float dW;        // max_j sum_i |W'_ij - W_ij|, W' = weights in the compute type
 };
@@ -95,6 +108,7 @@ struct NetDev {
     const float *mx0;        // [rows] max |y0|
     int layout;              // activation layout: 0 row-major, 1 MMA tiles, >= 2 row tiles (see act_index)
     int cc_compact;          // row-tile nets: 16-bit entries (input column only), every layer one weight value
+    int cc_split;            // row tiles of 2 rows split over the two CTAs of a cluster by feature (k_layer_cs)
     void *act[2];            // ping-pong activations, rows padded to a multiple of 128
     int32_t *cmap;           // [rows] compaction map: new row q <- output row cmap[q]
     int32_t *orig[2];        // list: original row id
@@ -184,10 +198,39 @@ __device__ __forceinline__ float z_error_bound(float e_in, float m_in, float S, 
 // Roundings per output of each fast kernel (see z_error_bound).
 __device__ __forceinline__ double fast_steps(const NetDev &n, const LayerDev &lw) {
     // CUDA-core kernels: one FMA rounding per term (zero-weight padding is
-    // exact) and one for the bias.  tcgen05:
+    // exact) and one for the bias; the feature-split kernel sums each half's
+    // terms (at most K - 1 of them when both halves have some) and adds the
+    // two sums, so a term still sees at most K + 1 roundings.  tcgen05:
     // accumulation order inside the MMA is not specified, so allow two
     // roundings for every product of every block plus the bias.
     return n.kernel == COSPDNN_KERNEL_TCGEN05 ? 2.0 * (16.0 * lw.max_blocks + 2.0) : (double)(lw.K + 2);
+}
+
+// Bound on |stored - clamped| for a value c in [0, 32] stored in the compute
+// type: half an ulp, at most 2^-11 c + 2^-25 (FP16; 2^-25 covers the
+// subnormal range) or 2^-8 c + 2^-126 (BF16, more than its subnormal half
+// spacing); 0 for FP32.
+template <typename T>
+__device__ __forceinline__ float store_error(float c) {
+    if constexpr (sizeof(T) == 4) return 0.0f;
+    else if constexpr (std::is_same<T, __half>::value) return __fmaf_ru(c, 4.8828125e-04f, 2.98023224e-08f);
+    else return __fmaf_ru(c, 3.90625e-03f, 1.17549435e-38f);
+}
+
+// Row statistics from the row's max pre-activation zm, its min |z - 16|
+// over the outputs (zd) and its error bound ez:
+//   max output  = the stored value of clamp(zm) (rounding is monotone, so
+//                 this is the max of the stored outputs);
+//   output error: outputs with z <= -ez are 0 in both recurrences and those
+//                 with z >= 32 + ez are 32 in both; the others, those with
+//                 |z - 16| < 16 + ez (there are some iff zd < 16 + ez), are
+//                 within ez of the exact clamp plus their storage rounding,
+//                 at most clamp(zm): bound ez + store_error(clamp(zm)), else 0.
+template <typename T>
+__device__ __forceinline__ void row_stats(float zm, float zd, float ez, float &emax, float &ymax) {
+    const float c = clamp32(zm);
+    ymax = act_traits<T>::to_f(act_traits<T>::from_f(c));
+    emax = zd < 16.0f + ez ? __fadd_ru(ez, store_error<T>(c)) : 0.0f;
 }
 
 }  // namespace cospdnn

@@ -457,7 +457,7 @@ constexpr int kCopyThreads = 256;
 // rows past the kept count zero.  The tile's row map is read once into
 // shared memory; threads then take the tile's feature columns in turn.
 // Kept rows are increasing, so a tile's rows come from a few consecutive
-// source tiles: when a feature column is one 8- or 16-byte piece, each
+// source tiles: when a feature column is one 4-, 8- or 16-byte piece, each
 // distinct source column is loaded once (one vector load, coalesced across
 // the threads of consecutive features) and the values are picked out of it;
 // wider columns move 16-byte destination pieces whose values are loaded one
@@ -478,7 +478,7 @@ __device__ __forceinline__ void copy_tile(const NetDev &nd, int q, int *s_map) {
         s_map[r] = row < R ? nd.cmap[row] : -1;
     }
     __syncthreads();
-    if (colb == 16 || colb == 8) {
+    if (colb == 16 || colb == 8 || colb == 4) {
         // TR <= 8 values per column: the map in registers
         int pm[kV];
 #pragma unroll
@@ -498,9 +498,11 @@ __device__ __forceinline__ void copy_tile(const NetDev &nd, int q, int *s_map) {
                     const E *c = src + ((t * N + f) << lg);
                     if (colb == 16) {
                         col = __ldg(reinterpret_cast<const uint4 *>(c));
-                    } else {
+                    } else if (colb == 8) {
                         const uint2 h = __ldg(reinterpret_cast<const uint2 *>(c));
                         col = make_uint4(h.x, h.y, 0u, 0u);
+                    } else {
+                        col = make_uint4(__ldg(reinterpret_cast<const uint32_t *>(c)), 0u, 0u, 0u);
                     }
                 }
                 const int off = (p & (TR - 1)) * (int)sizeof(E);  // byte offset in the column
@@ -513,7 +515,8 @@ __device__ __forceinline__ void copy_tile(const NetDev &nd, int q, int *s_map) {
                 }
             }
             if (colb == 16) *reinterpret_cast<uint4 *>(dst + ((int64_t)f << lg)) = *reinterpret_cast<const uint4 *>(v);
-            else *reinterpret_cast<uint2 *>(dst + ((int64_t)f << lg)) = *reinterpret_cast<const uint2 *>(v);
+            else if (colb == 8) *reinterpret_cast<uint2 *>(dst + ((int64_t)f << lg)) = *reinterpret_cast<const uint2 *>(v);
+            else *reinterpret_cast<uint32_t *>(dst + ((int64_t)f << lg)) = *reinterpret_cast<const uint32_t *>(v);
         }
         return;
     }

@@ -245,7 +245,9 @@ int cospdnn_engine_final_bound(cospdnn_engine *e, int net, float *max_bound, voi
 /* What the engine resolved for network `net` at build and did in its last
  * run: *kernel the layer kernel (COSPDNN_KERNEL_CUDA_CORE or _TCGEN05, never
  * AUTO), *row_tile the rows per activation tile of the CUDA-core row-tile
- * kernel (0 for the tcgen05 MMA-tile layout and the row-major gather kernel),
+ * kernel (0 for the tcgen05 MMA-tile layout and the row-major gather kernel;
+ * 2 for an FP16/BF16 net: the feature-split kernel, whose 2-row tiles are
+ * split by feature over the two CTAs of a cluster),
  * *layer0_counted 1 when layer 0 of the last run was computed by counting
  * the bits of a binary input.  Synchronizes `stream`. */
 int cospdnn_engine_net_info(cospdnn_engine *e, int net, int *kernel, int *row_tile,

@@ -54,20 +54,21 @@ def check_values(oracle, eng, nid, csc, y0, bias, layer, max_rows=512):
     return float(d.max())
 
 
-def test_65536_neurons_counted_layer0_and_tcgen05(cs, oracle):
+def test_65536_neurons_counted_layer0_and_feature_split(cs, oracle):
     """The C4 shape on 1024 rows x 120 layers: no row tile of 65536 FP16
-    features fits shared memory, so the engine takes tcgen05 and counts layer
-    0 from bit planes (k_layer0_bits16), then runs k_layer_tc."""
+    features fits one CTA's shared memory, so the engine splits 2-row tiles
+    by feature over the two CTAs of a cluster (k_layer_cs) and counts layer 0
+    from bit planes into 2-row tiles (k_layer0_bits16)."""
     csc, y0, b = make_net(65536, 120, 1024, seed=SEED, dlo=0.08, dhi=0.25)
     ref = oracle_run(csc, y0, b)
     eng, (nid,) = build(cs, [(csc, y0, b)], cs.PREC_FP16)
     eng.run()
     res = eng.result(nid)
     info = eng.net_info(nid)
-    assert info["kernel"] == cs.KERNEL_TCGEN05 and info["layer0_counted"]
+    assert info["kernel"] == cs.KERNEL_CUDA_CORE and info["row_tile"] == 2 and info["layer0_counted"]
     np.testing.assert_array_equal(res["alive"], ref["alive"])
     np.testing.assert_array_equal(res["categories"], ref["categories"])
-    assert ref["alive"][0] > 0  # layer 1 runs on the tcgen05 kernel
+    assert ref["alive"][0] > 0  # layer 1 runs on the split kernel
     dy0 = check_values(oracle, eng, nid, csc, y0, b, 0, max_rows=256)
     # layer 0 is counted exactly: the only error is the FP16 rounding of the output
     assert dy0 <= 32 * 2.0 ** -11
@@ -76,20 +77,60 @@ def test_65536_neurons_counted_layer0_and_tcgen05(cs, oracle):
     eng.close()
 
 
-def test_65536_neurons_bf16_forced_tcgen05_first_layer(cs, oracle):
-    """65536 neurons with layer 0 on the tcgen05 kernel as well (non-binary
-    FP32 inputs are not counted), BF16, 512 rows x 3 layers."""
-    csc, y0, b = make_net(65536, 3, 512, seed=SEED + 1, dlo=0.2, dhi=0.3)
-    rng = np.random.default_rng(3)
+def test_65536_neurons_sustained_feature_split_bf16_fp32_input(cs, oracle):
+    """Layer 0 on the split kernel as well (FP32 inputs are not counted),
+    BF16, 600 rows x 4 layers with denser inputs, so that rows survive into
+    layers 2 and 3; odd row count (the last 2-row tile has one row)."""
+    csc, y0, b = make_net(65536, 4, 601, seed=SEED + 3, dlo=0.3, dhi=0.45)
+    rng = np.random.default_rng(5)
     y0f = (y0 * rng.uniform(0.5, 1.5, size=y0.shape)).astype(np.float32)
     ref = oracle_run(csc, y0f, b)
     eng, (nid,) = build(cs, [(csc, y0f, b)], cs.PREC_BF16)
     eng.run()
     res = eng.result(nid)
-    assert not eng.net_info(nid)["layer0_counted"]
+    info = eng.net_info(nid)
+    assert info["row_tile"] == 2 and not info["layer0_counted"]
     np.testing.assert_array_equal(res["alive"], ref["alive"])
     np.testing.assert_array_equal(res["categories"], ref["categories"])
-    check_values(oracle, eng, nid, csc, y0f, b, 0, max_rows=128)
+    for l in range(4):
+        if ref["alive"][l] > 0:
+            check_values(oracle, eng, nid, csc, y0f, b, l, max_rows=128)
+    eng.close()
+
+
+def test_65536_neurons_feature_split_mixed_weights(cs, oracle):
+    """Weights of several values (no compact entry lists: column and weight
+    per entry) on the split kernel, FP16, 300 rows x 3 layers."""
+    csc, y0, b = make_net(65536, 3, 300, seed=SEED + 4, dlo=0.2, dhi=0.35)
+    rng = np.random.default_rng(9)
+    csc = [(cp, ri, (vv * rng.choice([0.5, 1.0, 1.5], size=vv.shape)).astype(np.float32)) for cp, ri, vv in csc]
+    ref = oracle_run(csc, y0, b)
+    eng, (nid,) = build(cs, [(csc, y0, b)], cs.PREC_FP16)
+    eng.run()
+    res = eng.result(nid)
+    assert eng.net_info(nid)["row_tile"] == 2
+    np.testing.assert_array_equal(res["alive"], ref["alive"])
+    np.testing.assert_array_equal(res["categories"], ref["categories"])
+    for l in range(3):
+        if ref["alive"][l] > 0:
+            check_values(oracle, eng, nid, csc, y0, b, l, max_rows=128)
+    eng.close()
+
+
+def test_65536_neurons_tcgen05_forced(cs, oracle):
+    """tcgen05 at 65536 neurons on request (layer 0 counted into MMA tiles,
+    then k_layer_tc), 512 rows x 6 layers."""
+    csc, y0, b = make_net(65536, 6, 512, seed=SEED, dlo=0.08, dhi=0.25)
+    ref = oracle_run(csc, y0, b)
+    eng, (nid,) = build(cs, [(csc, y0, b)], cs.PREC_FP16, kernel=cs.KERNEL_TCGEN05)
+    eng.run()
+    res = eng.result(nid)
+    info = eng.net_info(nid)
+    assert info["kernel"] == cs.KERNEL_TCGEN05 and info["layer0_counted"]
+    np.testing.assert_array_equal(res["alive"], ref["alive"])
+    np.testing.assert_array_equal(res["categories"], ref["categories"])
+    if ref["alive"][0] > 0:
+        check_values(oracle, eng, nid, csc, y0, b, 1, max_rows=128)
     eng.close()
 
 
