@@ -232,31 +232,37 @@ __global__ void __launch_bounds__(kBitsThreads, 2)
 constexpr int kBits16Threads = 512;
 constexpr int kBits16Warps = kBits16Threads / 32;
 
+// RT: feature-split nets (2-row tiles, the row-tile kernels' statistics);
+// else MMA-tile (tcgen05) nets.
+template <bool RT>
 __device__ __forceinline__ bool l0_net16(const NetDev &nd, int prec) {
-    return nd.l0_k > 0 && ((nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.layout == 1) || nd.cc_split) && nd.prec == prec &&
-           !nd.st->done && nd.st->layer == 0 && nd.y0bits != nullptr && *nd.y0nonbin == 0;
+    const bool kind = RT ? nd.cc_split != 0 : (nd.kernel == COSPDNN_KERNEL_TCGEN05 && nd.layout == 1);
+    return nd.l0_k > 0 && kind && nd.prec == prec && !nd.st->done && nd.st->layer == 0 && nd.y0bits != nullptr &&
+           *nd.y0nonbin == 0;
 }
 
-template <typename T>
+template <typename T, bool RT>
 __global__ void __launch_bounds__(kBits16Threads, 1)
     k_layer0_bits16(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
     count_launch(launches);
     extern __shared__ uint4 l0_smem[];
     uint16_t *s_w = reinterpret_cast<uint16_t *>(l0_smem);
-    __shared__ uint32_t s_zmax[16], s_emax[16];
+    // per row: max z; RT: min |z - 16| (bits of a value >= 0), else the
+    // tcgen05 epilogue's output error
+    __shared__ uint32_t s_zmax[16], s_zx[16];
     __shared__ float s_ez[16];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int n = 0; n < nnets; ++n) {
         const NetDev &nd = nets[n];
-        if (!l0_net16(nd, prec)) continue;
-        if (blockIdx.x == 0 && threadIdx.x == 0) nd.st->l0_bits = 1;  // the tcgen05 kernel skips layer 0
+        if (!l0_net16<RT>(nd, prec)) continue;
+        if (blockIdx.x == 0 && threadIdx.x == 0) nd.st->l0_bits = 1;  // the layer kernel skips layer 0
         const int N = nd.N, R = nd.st->R, K4 = nd.l0_k / 4;
         const int units = (R + 15) / 16, ngroups = N / 32;
         const LayerDev &lw = nd.layers[0];
         T *out = (T *)nd.act[nd.st->in_buf ^ 1];
         const float bias = nd.bias;
         for (int u = blockIdx.x; u < units; u += gridDim.x) {
-            __syncthreads();  // the previous unit is done with the words and the row maxima
+            __syncthreads();  // the previous unit is done with the words and the row statistics
             {
                 // half (u & 1) of the 32-row words of unit u / 2
                 const int sh = (u & 1) * 16;
@@ -269,88 +275,136 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                 }
                 if (threadIdx.x < 32) reinterpret_cast<uint32_t *>(s_w + N)[threadIdx.x] = 0u;  // padding
                 if (threadIdx.x < 16) {
-                    const int p = min(u * 16 + (int)threadIdx.x, R - 1);
                     s_zmax[threadIdx.x] = 0u;
-                    s_emax[threadIdx.x] = 0u;
-                    s_ez[threadIdx.x] =
-                        z_error_bound(nd.err[0][p], nd.mx[0][p], lw.S, lw.dW, bias, fast_steps(nd, lw));
+                    s_zx[threadIdx.x] = RT ? 0x7F800000u : 0u;  // +inf / 0
+                    if (!RT) {
+                        const int p = min(u * 16 + (int)threadIdx.x, R - 1);
+                        s_ez[threadIdx.x] =
+                            z_error_bound(nd.err[0][p], nd.mx[0][p], lw.S, lw.dW, bias, fast_steps(nd, lw));
+                    }
                 }
             }
             __syncthreads();
-            float zmx[16], ems[16], ezr[16];
+            float zmx[16], zx[16];
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
                 zmx[r] = -INFINITY;
-                ems[r] = 0.0f;
-                ezr[r] = s_ez[r];
+                zx[r] = RT ? INFINITY : 0.0f;
             }
-            for (int g = warp; g < ngroups; g += kBits16Warps) {
-                const int j = g * 32 + lane;
-                uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
-                const uint4 *ent = nd.l0_idx + (int64_t)g * K4 * 32 + lane;
-                for (int t = 0; t < K4; t += 4) {  // 16 entries, 8 packed words
-                    uint32_t x[8];
+            // blocks of 16 entries (4 x 16 bytes per lane) of the warp's groups in
+            // turn, the next block loaded while one is counted
+            uint32_t p[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+            uint4 qa[4], qb[4];
+            auto load = [&](uint4 *q, int g, int t) {
+                const uint4 *ent = nd.l0_idx + ((int64_t)g * K4 + t) * 32 + lane;
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) {
-                        const uint4 q = __ldg(ent + (int64_t)(t + v) * 32);
-                        x[2 * v] = (uint32_t)s_w[q.x] | ((uint32_t)s_w[q.y] << 16);
-                        x[2 * v + 1] = (uint32_t)s_w[q.z] | ((uint32_t)s_w[q.w] << 16);
-                    }
-                    add8(p, x);
+                for (int v = 0; v < 4; ++v) q[v] = __ldg(ent + v * 32);
+            };
+            auto count = [&](const uint4 *q) {
+                uint32_t x[8];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    x[2 * v] = (uint32_t)s_w[q[v].x] | ((uint32_t)s_w[q[v].y] << 16);
+                    x[2 * v + 1] = (uint32_t)s_w[q[v].z] | ((uint32_t)s_w[q[v].w] << 16);
                 }
-                const float w = nd.l0_w[j];
-                uint32_t c[8];
-                counts8(p, c);
-                T ov[16];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const uint32_t s2 = c[k] + (c[k] >> 16);  // even + odd entries' counts (each <= 32)
-                    float zz[2];
-                    z_pair(count_bits(s2, 0), count_bits(s2, 1), w, bias, zz[0], zz[1]);
-#pragma unroll
-                    for (int g = 0; g < 2; ++g) {
-                        const int r = 8 * g + k;
-                        const float z = zz[g];
-                        const float cz = clamp32(z);
-                        const T o = act_traits<T>::from_f(cz);
-                        zmx[r] = fmaxf(zmx[r], z);
-                        // the tcgen05 epilogue's error of an output near the clamp range
-                        if (z > -ezr[r] && z < 32.0f + ezr[r])
-                            ems[r] = fmaxf(ems[r], __fadd_ru(ezr[r], fabsf(act_traits<T>::to_f(o) - cz)));
-                        ov[r] = o;
-                    }
+                add8(p, x);
+            };
+            int g = warp, t = 0, par = 0;
+            if (g < ngroups) load(qa, g, 0);
+            while (g < ngroups) {
+                int gn = g, tn = t + 4;
+                if (tn >= K4) {
+                    tn = 0;
+                    gn += kBits16Warps;
                 }
-                if (nd.layout == 1) {
-#pragma unroll
-                    for (int r = 0; r < 16; ++r) out[act_index(1, N, (int64_t)u * 16 + r, j)] = ov[r];
+                if (par == 0) {
+                    if (gn < ngroups) load(qb, gn, tn);
+                    count(qa);
                 } else {
-                    // 2-row tiles (feature-split nets): one 4-byte word per row pair,
-                    // consecutive outputs adjacent
-#pragma unroll
-                    for (int r = 0; r < 16; r += 2)
-                        *reinterpret_cast<uint32_t *>(out + act_index(2, N, (int64_t)u * 16 + r, j)) =
-                            (uint32_t)*reinterpret_cast<const uint16_t *>(&ov[r]) |
-                            ((uint32_t)*reinterpret_cast<const uint16_t *>(&ov[r + 1]) << 16);
+                    if (gn < ngroups) load(qa, gn, tn);
+                    count(qb);
                 }
+                par ^= 1;
+                if (tn == 0) {
+                    // group g counted: outputs of its 16 rows
+                    const int j = g * 32 + lane;
+                    const float w = nd.l0_w[j];
+                    uint32_t c[8];
+                    counts8(p, c);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) p[k] = 0u;
+                    T ov[16];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t s2 = c[k] + (c[k] >> 16);  // even + odd entries' counts (each <= 32)
+                        float zz[2];
+                        z_pair(count_bits(s2, 0), count_bits(s2, 1), w, bias, zz[0], zz[1]);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int r = 8 * h + k;
+                            const float z = zz[h];
+                            const float cz = clamp32(z);
+                            ov[r] = act_traits<T>::from_f(cz);
+                            zmx[r] = fmaxf(zmx[r], z);
+                            if constexpr (RT) {
+                                zx[r] = fminf(zx[r], fabsf(z - 16.0f));
+                            } else {
+                                // the tcgen05 epilogue's error of an output near the clamp range
+                                const float ez = s_ez[r];
+                                if (z > -ez && z < 32.0f + ez)
+                                    zx[r] = fmaxf(zx[r], __fadd_ru(ez, fabsf(act_traits<T>::to_f(ov[r]) - cz)));
+                            }
+                        }
+                    }
+                    if constexpr (RT) {
+                        // 2-row tiles: one 4-byte word per row pair, consecutive outputs adjacent
+#pragma unroll
+                        for (int r = 0; r < 16; r += 2)
+                            *reinterpret_cast<uint32_t *>(out + act_index(2, N, (int64_t)u * 16 + r, j)) =
+                                (uint32_t)*reinterpret_cast<const uint16_t *>(&ov[r]) |
+                                ((uint32_t)*reinterpret_cast<const uint16_t *>(&ov[r + 1]) << 16);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < 16; ++r) out[act_index(1, N, (int64_t)u * 16 + r, j)] = ov[r];
+                    }
+                }
+                g = gn;
+                t = tn;
             }
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
                 const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
-                const uint32_t e = __reduce_max_sync(0xffffffffu, __float_as_uint(ems[r]));  // >= 0
-                if (lane == r) {
-                    atomicMax(&s_zmax[r], m);
-                    atomicMax(&s_emax[r], e);
+                if constexpr (RT) {
+                    const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zx[r]));  // >= 0
+                    if (lane == r) {
+                        atomicMax(&s_zmax[r], m);
+                        atomicMin(&s_zx[r], d);
+                    }
+                } else {
+                    const uint32_t e = __reduce_max_sync(0xffffffffu, __float_as_uint(zx[r]));  // >= 0
+                    if (lane == r) {
+                        atomicMax(&s_zmax[r], m);
+                        atomicMax(&s_zx[r], e);
+                    }
                 }
             }
             __syncthreads();
             if (threadIdx.x < 16) {
-                const int p = u * 16 + threadIdx.x;
-                if (p < R) {
-                    const float c = clamp32(ord2f(s_zmax[threadIdx.x]));
-                    const float ym = act_traits<T>::to_f(act_traits<T>::from_f(c));  // the max stored output
-                    atomicMax(&nd.stat[3 * p], s_zmax[threadIdx.x]);
-                    atomicMax(&nd.stat[3 * p + 1], s_emax[threadIdx.x]);
-                    atomicMax(&nd.stat[3 * p + 2], __float_as_uint(ym));
+                const int pr = u * 16 + threadIdx.x;
+                if (pr < R) {
+                    float em, ym;
+                    if constexpr (RT) {
+                        const float ez = z_error_bound(nd.err[0][pr], nd.mx[0][pr], lw.S, lw.dW, bias,
+                                                       fast_steps(nd, lw));
+                        row_stats<T>(ord2f(s_zmax[threadIdx.x]), __uint_as_float(s_zx[threadIdx.x]), ez, em, ym);
+                    } else {
+                        const float c = clamp32(ord2f(s_zmax[threadIdx.x]));
+                        ym = act_traits<T>::to_f(act_traits<T>::from_f(c));  // the max stored output
+                        em = __uint_as_float(s_zx[threadIdx.x]);
+                    }
+                    atomicMax(&nd.stat[3 * pr], s_zmax[threadIdx.x]);
+                    atomicMax(&nd.stat[3 * pr + 1], __float_as_uint(em));
+                    atomicMax(&nd.stat[3 * pr + 2], __float_as_uint(ym));
                 }
             }
         }
@@ -607,17 +661,19 @@ int l0_build(const std::vector<int32_t> &colptr, const std::vector<int32_t> &row
     return 0;
 }
 
-int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, bool mma, unsigned long long *launches, int sms,
+int l0_spec(KSpec &k, NetDev *nets, int nnets, int prec, int kind, unsigned long long *launches, int sms,
             int max_n) {
     using F = void (*)(const NetDev *, int, int, unsigned long long *);
     static const F fns[3] = {k_layer0_bits<float>, k_layer0_bits<__half>, k_layer0_bits<__nv_bfloat16>};
-    static const F fns16[3] = {nullptr, k_layer0_bits16<__half>, k_layer0_bits16<__nv_bfloat16>};
-    CSP_CHECK(!mma || prec != COSPDNN_PREC_FP32, COSPDNN_ERR_UNSUPPORTED, "l0_spec: FP32 MMA-tile net");
-    k.fn = (void *)(mma ? fns16[prec] : fns[prec]);
-    k.smem = mma ? (size_t)(max_n + 64) * 2 : (size_t)(max_n + 32) * 4;
+    static const F fns16[2][3] = {{nullptr, k_layer0_bits16<__half, false>, k_layer0_bits16<__nv_bfloat16, false>},
+                                  {nullptr, k_layer0_bits16<__half, true>, k_layer0_bits16<__nv_bfloat16, true>}};
+    const bool sixteen = kind != kL0Rows32;
+    CSP_CHECK(!sixteen || prec != COSPDNN_PREC_FP32, COSPDNN_ERR_UNSUPPORTED, "l0_spec: FP32 16-row net");
+    k.fn = (void *)(sixteen ? fns16[kind == kL0Split16 ? 1 : 0][prec] : fns[prec]);
+    k.smem = sixteen ? (size_t)(max_n + 64) * 2 : (size_t)(max_n + 32) * 4;
     CSP_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
-    k.grid = dim3(mma ? sms : 2 * sms);
-    k.block = dim3(mma ? kBits16Threads : kBitsThreads);
+    k.grid = dim3(sixteen ? sms : 2 * sms);
+    k.block = dim3(sixteen ? kBits16Threads : kBitsThreads);
     k.arg(nets).arg(nnets).arg(prec).arg(launches);
     return COSPDNN_OK;
 }

@@ -164,13 +164,14 @@ __device__ __forceinline__ void cs_group(float &a0, float &a1, uint4 q, uint32_t
 
 // Bounded wait on a phase of one of this CTA's mbarriers.  False when this
 // CTA has aborted: the limit ran out here or in another thread of the CTA.
-__device__ __forceinline__ bool cs_wait(uint32_t bar, uint32_t parity, long long limit, volatile int *abort) {
+__device__ __forceinline__ bool cs_wait(uint32_t bar, uint32_t parity, const volatile long long *limit,
+                                        volatile int *abort) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         if (*abort) return false;
         if (mbar_try_wait(bar, parity)) return true;
-        if (clock64() - t0 > limit) {
+        if (clock64() - t0 > *limit) {
             *abort = 1;
             return false;
         }
@@ -195,15 +196,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kCsThreads, 1)
     __shared__ __align__(8) unsigned long long s_full[kCsDepth], s_empty[kCsDepth];
     __shared__ uint32_t s_zmax[2], s_zdist[2];
     __shared__ int s_abort;
+    __shared__ long long s_limit;
+    __shared__ int s_withhold;  // test hook: CTA 0 of cluster 0 does not send its first message
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t rank = cluster_rank(), peer = rank ^ 1u;
-    const long long limit = limits->wait_cycles;
     if (tid == 0) {
         for (int d = 0; d < kCsDepth; ++d) {
             mbar_init(smem_addr(&s_full[d]), 1);
             mbar_init(smem_addr(&s_empty[d]), kCsWarps);
         }
         s_abort = 0;
+        s_limit = limits->wait_cycles;
+        s_withhold = limits->withhold_stage && rank == 0 && cluster_id() == 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         // the first phase of each receive buffer: this CTA's arrive plus the
         // peer's messages
@@ -299,17 +303,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kCsThreads, 1)
         float own[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // owned partials of the round awaiting the peer's message
         int own_k = -1;                            // that round (-1: none)
         uint32_t own_rc = 0;
+        // this CTA's slot s' is slot s' ^ rank: its own slots are always 0 and
+        // 2, the ones it sends 1 and 3
+        const int sw = rank ? 32 : 0;
         auto load_col = [&](uint4 *q, int k, int t) {
             const uint4 *p = E + (int64_t)((kCsWarps * k + warp) * cnt + t) * (kCsSlots * 32);
-#pragma unroll
-            for (int s = 0; s < kCsSlots; ++s) q[s] = __ldg(p + s * 32);
+            q[0] = __ldg(p + sw);
+            q[1] = __ldg(p + 32 - sw);
+            q[2] = __ldg(p + 64 + sw);
+            q[3] = __ldg(p + 96 - sw);
         };
         // the owner's half of a round: wait for the peer's message, add, bias,
         // clamp, store, row statistics; then hand the buffer back
         auto finish = [&]() {
             const uint32_t d = own_rc & 1u;
             uint4 m = make_uint4(0u, 0u, 0u, 0u);
-            if (ok) ok = cs_wait(smem_addr(&s_full[d]), (own_rc >> 1) & 1u, limit, abort_p);
+            if (ok) ok = cs_wait(smem_addr(&s_full[d]), (own_rc >> 1) & 1u, &s_limit, abort_p);
             if (ok) {
                 asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
                              : "=r"(m.x), "=r"(m.y), "=r"(m.z), "=r"(m.w)
@@ -341,21 +350,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kCsThreads, 1)
         // previous round, keep this round's owned pairs
         auto round_end = [&](int k) {
             const uint32_t d = rc & 1u;
-            const int sp = (int)peer;  // the peer owns slots sp and sp + 2
-            const float a0 = sp ? acc[1][0] : acc[0][0], a1 = sp ? acc[1][1] : acc[0][1];
-            const float a2 = sp ? acc[3][0] : acc[2][0], a3 = sp ? acc[3][1] : acc[2][1];
-            const uint4 msg = make_uint4(__float_as_uint(a0), __float_as_uint(a1), __float_as_uint(a2),
-                                         __float_as_uint(a3));
+            const uint4 msg = make_uint4(__float_as_uint(acc[1][0]), __float_as_uint(acc[1][1]),
+                                         __float_as_uint(acc[3][0]), __float_as_uint(acc[3][1]));
             if (ok && rc >= (uint32_t)kCsDepth)  // the peer has read this buffer's previous message
-                ok = cs_wait(smem_addr(&s_empty[d]), ((rc >> 1) - 1u) & 1u, limit, abort_p);
-            if (ok)
+                ok = cs_wait(smem_addr(&s_empty[d]), ((rc >> 1) - 1u) & 1u, &s_limit, abort_p);
+            if (ok && !(rc == 0 && s_withhold))
                 st_async16(peer_recv + (d * kCsThreads + tid) * kCsMsgBytes, msg,
                            peer_addr(smem_addr(&s_full[d]), peer));
             if (own_k >= 0) finish();
-            own[0] = sp ? acc[0][0] : acc[1][0];
-            own[1] = sp ? acc[0][1] : acc[1][1];
-            own[2] = sp ? acc[2][0] : acc[3][0];
-            own[3] = sp ? acc[2][1] : acc[3][1];
+            own[0] = acc[0][0];
+            own[1] = acc[0][1];
+            own[2] = acc[2][0];
+            own[3] = acc[2][1];
             own_k = k;
             own_rc = rc++;
 #pragma unroll

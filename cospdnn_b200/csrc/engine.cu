@@ -497,15 +497,16 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
         if (rc) return rc;
         e->layer_specs.push_back(std::move(k));
     }
-    for (int mma = 0; mma < 2; ++mma)
+    for (int kind : {kL0Rows32, kL0Mma16, kL0Split16})
         for (int prec = 0; prec < 3; ++prec) {
             int max_n = 0;
-            for (const Net &n : e->nets)
-                if (n.dev.l0_k > 0 && n.d.precision == prec && (n.dev.layout == 1 || n.dev.cc_split) == (mma == 1))
-                    max_n = std::max(max_n, n.d.neuron);
+            for (const Net &n : e->nets) {
+                const int nk = n.dev.cc_split ? kL0Split16 : n.dev.layout == 1 ? kL0Mma16 : kL0Rows32;
+                if (n.dev.l0_k > 0 && n.d.precision == prec && nk == kind) max_n = std::max(max_n, n.d.neuron);
+            }
             if (!max_n) continue;
             KSpec k;
-            int rc = l0_spec(k, nets, nn, prec, mma == 1, launches, sms, max_n);
+            int rc = l0_spec(k, nets, nn, prec, kind, launches, sms, max_n);
             if (rc) return rc;
             e->l0_specs.push_back(std::move(k));
         }

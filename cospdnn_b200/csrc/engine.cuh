@@ -140,9 +140,10 @@ enum { CLS_PRUNE = 0, CLS_KEEP = 1, CLS_UNCERTAIN = 2 };
 // them between runs so that tests can make a bounded wait or the loop guard
 // run out and check the error path).
 struct DevLimits {
-    long long wait_cycles;  // bounded mbarrier waits of k_layer_tc (SM clock cycles)
+    long long wait_cycles;  // bounded mbarrier waits of k_layer_tc and k_layer_cs (SM clock cycles)
     int max_iters;          // layer-loop iterations before the guard stops the run
-    int withhold_stage;     // 1: CTA 0 of k_layer_tc issues no copy for its first stage
+    int withhold_stage;     // 1: CTA 0 of k_layer_tc issues no copy for its first stage, and CTA 0 of
+                            // k_layer_cs's first cluster does not send its first partial sums
 };
 constexpr long long kDefaultWaitCycles = 4000000000LL;  // about 2 s at 1.9 GHz
 

@@ -258,13 +258,15 @@ int cospdnn_engine_net_info(cospdnn_engine *e, int net, int *kernel, int *row_ti
  * iteration guard; when one runs out the run stops and
  * cospdnn_engine_result returns COSPDNN_ERR_DEVICE, and the next run starts
  * clean.  These set, for the following runs: wait_cycles, the limit of each
- * bounded wait of the tcgen05 layer kernel in SM clock cycles (0 = the
- * default of 4e9, about 2 s; values below 1e6 are rejected); max_iters, the
- * layer-loop iterations after which the guard stops the run (0 = the default
- * of the deepest network's layers + 2); withhold_stage = 1 makes the first
- * block of the tcgen05 layer kernel skip the copies of its first stage, so
- * that its wait for them runs out (a copy that never arrives, made on
- * purpose; no fault, no hang).  (0, 0, 0) restores the defaults.
+ * bounded wait of the tcgen05 and feature-split layer kernels in SM clock
+ * cycles (0 = the default of 4e9, about 2 s; values below 1e6 are rejected);
+ * max_iters, the layer-loop iterations after which the guard stops the run
+ * (0 = the default of the deepest network's layers + 2); withhold_stage = 1
+ * makes the first block of the tcgen05 layer kernel skip the copies of its
+ * first stage, and the first block of the feature-split kernel skip its
+ * first message to the other block of its cluster, so that the waits for
+ * them run out (data that never arrives, made on purpose; no fault, no
+ * hang).  (0, 0, 0) restores the defaults.
  * Synchronizes the device. */
 int cospdnn_engine_set_test_limits(cospdnn_engine *e, long long wait_cycles, int max_iters,
                                    int withhold_stage);

@@ -4,7 +4,8 @@ Every wait of the engine's kernels is bounded and the layer loop has an
 iteration guard.  These tests make one of them run out on purpose through
 the engine's test hooks (cospdnn_engine_set_test_limits): a copy that the
 tcgen05 kernel's producer never issues (its consumer's bounded wait gives up
-after about 10 ms), and a loop guard of two iterations.  The run then stops,
+after about 10 ms), a message that one CTA of the feature-split kernel's
+cluster never sends to the other, and a loop guard of two iterations.  The run then stops,
 the result call reports COSPDNN_ERR_DEVICE, and the next run with the default
 limits is clean and exact against the FP64 oracle.  Nothing traps, faults or
 hangs: the kernels return and the context stays usable."""
@@ -87,6 +88,31 @@ def test_loop_guard_stops_the_run(cs):
     assert len(ms) == 3
     with pytest.raises(cs.CospdnnError):
         eng.result(nid)
+    eng.set_test_limits()
+    eng.run()
+    res = eng.result(nid)
+    np.testing.assert_array_equal(res["alive"], ref["alive"])
+    np.testing.assert_array_equal(res["categories"], ref["categories"])
+    eng.close()
+
+
+def test_feature_split_wait_for_a_withheld_message_runs_out(cs):
+    """65536 neurons take the feature-split kernel (two CTAs of a cluster
+    exchange partial sums): the first CTA of the first cluster skips its
+    first message, the other CTA's bounded wait for it runs out, then the
+    first CTA's wait for the buffer's release; both stop and meet at the
+    cluster barrier, the run reports COSPDNN_ERR_DEVICE, and the next run
+    with the default limits is exact."""
+    csc, y0, b = make_net(65536, 3, 600, seed=75, dlo=0.08, dhi=0.25)
+    ref = oracle_run(csc, y0, b)
+    assert ref["alive"][0] > 0  # layer 1 runs on the split kernel
+    eng, nid = build(cs, csc, y0, b, cs.PREC_FP16, cs.KERNEL_AUTO)
+    assert eng.net_info(nid)["row_tile"] == 2
+    eng.set_test_limits(wait_cycles=WAIT, withhold_stage=1)
+    eng.run()
+    with pytest.raises(cs.CospdnnError) as e:
+        eng.result(nid)
+    assert e.value.code == cs.ERR_DEVICE
     eng.set_test_limits()
     eng.run()
     res = eng.result(nid)
