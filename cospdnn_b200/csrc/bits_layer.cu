@@ -64,6 +64,19 @@ __device__ __forceinline__ void z_pair(uint32_t c0, uint32_t c1, float w, float 
         : "r"(c0), "r"(c1), "f"(w), "f"(bias), "f"(-8388608.0f));
 }
 
+// Two values as the 16-bit pair word {lo, hi} of type T, each max(v, 0)
+// rounded to nearest (one cvt.rn.relu: the same values as from_f(fmaxf(v, 0))).
+__device__ __forceinline__ uint32_t relu_pack(float lo, float hi, __half) {
+    uint32_t d;
+    asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+__device__ __forceinline__ uint32_t relu_pack(float lo, float hi, __nv_bfloat16) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
 template <typename T>
 struct Pack;
 template <>
@@ -309,14 +322,20 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                 }
                 add8(p, x);
             };
+            const bool small = RT && nd.l0_small != 0;
             int g = warp, t = 0, par = 0;
-            if (g < ngroups) load(qa, g, 0);
+            float w = 0.0f, wn = 0.0f;  // weight of the group being counted, of the next one
+            if (g < ngroups) {
+                load(qa, g, 0);
+                w = __ldg(nd.l0_w + g * 32 + lane);
+            }
             while (g < ngroups) {
                 int gn = g, tn = t + 4;
                 if (tn >= K4) {
                     tn = 0;
                     gn += kBits16Warps;
                 }
+                if (tn == 0 && gn < ngroups) wn = __ldg(nd.l0_w + gn * 32 + lane);
                 if (par == 0) {
                     if (gn < ngroups) load(qb, gn, tn);
                     count(qa);
@@ -325,10 +344,32 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                     count(qb);
                 }
                 par ^= 1;
-                if (tn == 0) {
+                if (tn == 0 && small) {
+                    // every output |z| <= 16: no clamp at 32, min |z - 16| from the
+                    // row max; row pairs (r, r + 1) converted and packed at once
+                    const int j = g * 32 + lane;
+                    uint32_t c[8];
+                    counts8(p, c);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) p[k] = 0u;
+#pragma unroll
+                    for (int k = 0; k < 8; k += 2) {
+                        const uint32_t sa = c[k] + (c[k] >> 16), sb = c[k + 1] + (c[k + 1] >> 16);
+                        float za[2], zb[2];  // rows (k, 8 + k), (k + 1, 9 + k)
+                        z_pair(count_bits(sa, 0), count_bits(sa, 1), w, bias, za[0], za[1]);
+                        z_pair(count_bits(sb, 0), count_bits(sb, 1), w, bias, zb[0], zb[1]);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int r = 8 * h + k;
+                            zmx[r] = fmaxf(zmx[r], za[h]);
+                            zmx[r + 1] = fmaxf(zmx[r + 1], zb[h]);
+                            *reinterpret_cast<uint32_t *>(out + act_index(2, N, (int64_t)u * 16 + r, j)) =
+                                relu_pack(za[h], zb[h], T());
+                        }
+                    }
+                } else if (tn == 0) {
                     // group g counted: outputs of its 16 rows
                     const int j = g * 32 + lane;
-                    const float w = nd.l0_w[j];
                     uint32_t c[8];
                     counts8(p, c);
 #pragma unroll
@@ -368,6 +409,7 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                         for (int r = 0; r < 16; ++r) out[act_index(1, N, (int64_t)u * 16 + r, j)] = ov[r];
                     }
                 }
+                if (tn == 0) w = wn;
                 g = gn;
                 t = tn;
             }
@@ -375,10 +417,10 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
             for (int r = 0; r < 16; ++r) {
                 const uint32_t m = __reduce_max_sync(0xffffffffu, f2ord(zmx[r]));
                 if constexpr (RT) {
-                    const uint32_t d = __reduce_min_sync(0xffffffffu, __float_as_uint(zx[r]));  // >= 0
+                    const uint32_t d = small ? 0x7F800000u : __reduce_min_sync(0xffffffffu, __float_as_uint(zx[r]));
                     if (lane == r) {
                         atomicMax(&s_zmax[r], m);
-                        atomicMin(&s_zx[r], d);
+                        if (!small) atomicMin(&s_zx[r], d);  // >= 0: bit order = value order
                     }
                 } else {
                     const uint32_t e = __reduce_max_sync(0xffffffffu, __float_as_uint(zx[r]));  // >= 0
@@ -396,7 +438,10 @@ __global__ void __launch_bounds__(kBits16Threads, 1)
                     if constexpr (RT) {
                         const float ez = z_error_bound(nd.err[0][pr], nd.mx[0][pr], lw.S, lw.dW, bias,
                                                        fast_steps(nd, lw));
-                        row_stats<T>(ord2f(s_zmax[threadIdx.x]), __uint_as_float(s_zx[threadIdx.x]), ez, em, ym);
+                        const float zm = ord2f(s_zmax[threadIdx.x]);
+                        // |z| <= 16: min |z - 16| is |max z - 16| (rounding of z - 16 is monotone)
+                        const float zd = small ? fabsf(zm - 16.0f) : __uint_as_float(s_zx[threadIdx.x]);
+                        row_stats<T>(zm, zd, ez, em, ym);
                     } else {
                         const float c = clamp32(ord2f(s_zmax[threadIdx.x]));
                         ym = act_traits<T>::to_f(act_traits<T>::from_f(c));  // the max stored output
