@@ -252,6 +252,71 @@ __device__ __forceinline__ void cc_store(float *acc, float *zmax, float *zdist, 
     else *reinterpret_cast<uint2 *>(dst) = *reinterpret_cast<const uint2 *>(ov);
 }
 
+// Staging of a row tile whose rows come through the compaction map (the
+// previous layer pruned rows and left the copy to this kernel): row r of the
+// tile <- row s_map[r] of the whole buffer `src` (-1: zero).  Kept rows are
+// increasing, so a tile's rows come from a few consecutive source tiles: for
+// 8- and 16-byte feature columns each row's source column is loaded (the
+// loads independent, repeats served by L1) and its value picked out; wider
+// columns are built one 16-byte piece at a time from single values.
+template <typename E, int NT>
+__device__ __forceinline__ void cc_stage_gather(const E *__restrict__ src, int N, int TR, const int *s_map,
+                                                uint4 *smem) {
+    constexpr int kV = 16 / (int)sizeof(E);  // values of a 16-byte piece
+    const int lg = __ffs(TR) - 1;            // TR is a power of two
+    const int colb = TR * (int)sizeof(E);
+    if (colb == 16 || colb == 8) {
+        int pm[kV];
+#pragma unroll
+        for (int i = 0; i < kV; ++i) pm[i] = i < TR ? s_map[i] : -1;
+        for (int f = threadIdx.x; f < N; f += NT) {
+            // every row's source column loaded independently (repeats of a
+            // column hit L1), then the values picked out
+            uint4 col[kV];
+#pragma unroll
+            for (int i = 0; i < kV; ++i) {
+                const int p = pm[i];
+                col[i] = make_uint4(0u, 0u, 0u, 0u);
+                if (p < 0) continue;
+                const E *c = src + (((int64_t)(p >> lg) * N + f) << lg);
+                if (colb == 16) {
+                    col[i] = __ldg(reinterpret_cast<const uint4 *>(c));
+                } else {
+                    const uint2 h = __ldg(reinterpret_cast<const uint2 *>(c));
+                    col[i] = make_uint4(h.x, h.y, 0u, 0u);
+                }
+            }
+            __align__(16) E v[kV];
+#pragma unroll
+            for (int i = 0; i < kV; ++i) {
+                const int p = pm[i];
+                const int off = (p & (TR - 1)) * (int)sizeof(E);  // byte offset in the column
+                const uint32_t w = off < 8 ? (off < 4 ? col[i].x : col[i].y) : (off < 12 ? col[i].z : col[i].w);
+                if constexpr (sizeof(E) == 4) {
+                    v[i] = p < 0 ? E(0) : __uint_as_float(w);
+                } else {
+                    v[i] = p < 0 ? E(0) : (E)(w >> (8 * (off & 3)));
+                }
+            }
+            if (colb == 16) smem[f] = *reinterpret_cast<const uint4 *>(v);
+            else reinterpret_cast<uint2 *>(smem)[f] = *reinterpret_cast<const uint2 *>(v);
+        }
+        return;
+    }
+    const int lp = lg - (__ffs(kV) - 1);  // log2 of 16-byte pieces per column
+    const int total = N << lp;
+    for (int u = threadIdx.x; u < total; u += NT) {
+        const int f = u >> lp, pc = u & ((1 << lp) - 1);
+        __align__(16) E v[kV];
+#pragma unroll
+        for (int i = 0; i < kV; ++i) {
+            const int p = s_map[pc * kV + i];
+            v[i] = p < 0 ? E(0) : src[(((int64_t)(p >> lg) * N + f) << lg) + (p & (TR - 1))];
+        }
+        smem[u] = *reinterpret_cast<const uint4 *>(v);
+    }
+}
+
 template <typename T, int NT, int LB, bool CMP>
 __global__ void __launch_bounds__(NT, 512 / NT)
     k_layer_cc(const NetDev *__restrict__ nets, int nnets, int prec, unsigned long long *launches) {
@@ -262,6 +327,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
     constexpr int kRing = cc_ring<T>();
     extern __shared__ uint4 cc_smem[];
     __shared__ uint32_t s_zmax[kCcMaxTR], s_zdist[kCcMaxTR];
+    __shared__ int s_map[kCcMaxTR];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grid = (int)gridDim.x;
     int64_t total = 0;
@@ -284,7 +350,15 @@ __global__ void __launch_bounds__(NT, 512 / NT)
 
         // ---- stage the tile in shared memory
         __syncthreads();  // the previous item is done with the tile and s_zmax
-        {
+        if (nd.st->gather) {
+            for (int r = threadIdx.x; r < TR; r += NT) {
+                const int q = it.tile * TR + r;
+                s_map[r] = q < R ? nd.cmap[q] : -1;
+            }
+            __syncthreads();
+            if constexpr (ES == 4) cc_stage_gather<float, NT>((const float *)in, N, TR, s_map, cc_smem);
+            else cc_stage_gather<uint16_t, NT>((const uint16_t *)in, N, TR, s_map, cc_smem);
+        } else {
             const uint4 *src = reinterpret_cast<const uint4 *>(in + (int64_t)it.tile * N * TR);
             const int nvec = N * TR * ES / 16;
             int i = threadIdx.x;
@@ -296,7 +370,10 @@ __global__ void __launch_bounds__(NT, 512 / NT)
                 for (int k = 0; k < 8; ++k) cc_smem[i + k * NT] = v[k];
             }
             for (; i < nvec; i += NT) cc_smem[i] = __ldg(src + i);
+        }
+        {
             // the zero columns after the N inputs (read by padding entries)
+            const int nvec = N * TR * ES / 16;
             for (int z = threadIdx.x; z < kCcZeroCols * TR * ES / 16; z += NT)
                 cc_smem[nvec + z] = make_uint4(0u, 0u, 0u, 0u);
             for (int r = threadIdx.x; r < TR; r += NT) {
@@ -308,7 +385,7 @@ __global__ void __launch_bounds__(NT, 512 / NT)
             // the next tile of this CTA into L2 while this one is computed
             CcItem nx;
             if (cc_locate(nets, nnets, prec, LB, CMP, grid, kWarps, item + grid, nx) &&
-                (nx.net != it.net || nx.tile != it.tile)) {
+                (nx.net != it.net || nx.tile != it.tile) && !nets[nx.net].st->gather) {
                 const NetDev &nn = nets[nx.net];
                 const T *nin = (const T *)(nn.st->layer == 0 ? nn.y0 : nn.act[nn.st->in_buf]);
                 const uint32_t bytes = (uint32_t)((size_t)nn.N * nn.layout * ES);

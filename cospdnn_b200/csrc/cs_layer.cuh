@@ -13,7 +13,7 @@ namespace cospdnn {
 bool cs_supported(int N, int prec);
 // Builds one layer's split entry lists from its CSC (split bit chosen per
 // layer, conflict-free order per half and group of 32 outputs) and uploads
-// them; compact: 16-bit entries (the layer has one weight value).
+// them; compact: entries without a weight (the layer has one weight value).
 int cs_build_entries(const std::vector<int32_t> &colptr, const std::vector<int32_t> &rowidx,
                      const std::vector<float> &vals, int N, int prec, bool compact, LayerDev &ld,
                      std::vector<void *> &owned);

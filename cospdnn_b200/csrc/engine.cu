@@ -232,9 +232,11 @@ __global__ void k_gather_rows(const NetDev *__restrict__ nd_p, float *__restrict
     const T *act = (const T *)nd.act[nd.st->in_buf];
     const int64_t rows = min((int64_t)R, max_rows), total = rows * N;
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (int64_t)gridDim.x * blockDim.x;
+    const bool gather = nd.st->gather != 0;  // row q is row cmap[q] of the buffer (compaction pending)
     for (int64_t i = tid; i < total; i += nth) {
         const int64_t q = i / N, j = i % N;
-        out[i] = act_traits<T>::to_f(act[act_index(nd.layout, N, q, (int)j)]);
+        const int64_t src = gather ? nd.cmap[q] : q;
+        out[i] = act_traits<T>::to_f(act[act_index(nd.layout, N, src, (int)j)]);
     }
     // the row lists of the next layer: original ids, and the proven bound on
     // |Y(fast) - Y(FP64)| of these values
@@ -532,7 +534,11 @@ int make_specs(cospdnn_engine *e, const KernelSets &ks) {
     k3.fn = (void *)k_replay;
     k3.grid = dim3(e->replay_ctas);
     k3.block = dim3(kReplayThreads);
-    k3.smem = sizeof(double) * 2 * (size_t)std::min(e->max_n, kReplaySmemN);
+    {
+        int sd = 0;
+        for (const Net &n : e->nets) sd = std::max(sd, replay_smem_doubles(n.d.neuron));
+        k3.smem = sizeof(double) * (size_t)sd;
+    }
     CSP_CUDA(cudaFuncSetAttribute(k3.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k3.smem));
     k3.arg(nets).arg(nn).arg(e->scratch).arg(e->max_n).arg(launches);
     KSpec &k5 = e->k5;

@@ -95,6 +95,8 @@ struct NetState {
     int in_buf;  // act[in_buf] is the input of `layer` (layer 0 reads y0)
     int copy_R;  // rows the pending compaction copies (0 = none pending)
     int l0_bits; // layer 0 of this run was computed by the bit-count kernel
+    int gather;  // input row q of `layer` is row cmap[q] of act[in_buf] (row-tile nets: the
+                 // layer kernel's staging does the compaction, no copy)
 };
 
 struct NetDev {
