@@ -443,6 +443,24 @@ int upload_layer(cospdnn_engine *e, Net &net, int l, LayerDev &ld) {
     ld.K = K;
     ld.S = (float)(S * (1.0 + 1e-7));
     ld.dW = (float)(dW * (1.0 + 1e-7));
+    // entries for the FP64 replay in a quarter of the bytes when the layer
+    // has one weight value: 16-bit indices, that value held once
+    bool one = N <= 65536 && K <= 65535 && h.colptr[N] > 0;
+    for (int64_t p = 1; one && p < h.colptr[N]; ++p) one = h.vals[p] == h.vals[0];
+    if (one) {
+        std::vector<uint16_t> ri((size_t)K * N, 0), rc(N);
+        for (int j = 0; j < N; ++j) {
+            rc[j] = (uint16_t)(h.colptr[j + 1] - h.colptr[j]);
+            for (int p = h.colptr[j], k = 0; p < h.colptr[j + 1]; ++p, ++k) ri[(size_t)k * N + j] = (uint16_t)h.rowidx[p];
+        }
+        uint16_t *dri = dalloc<uint16_t>(ri.size(), e->owned), *drc = dalloc<uint16_t>(rc.size(), e->owned);
+        CSP_CHECK(dri && drc, COSPDNN_ERR_NOMEM, "engine: weight allocation failed");
+        CSP_CUDA(cudaMemcpy(dri, ri.data(), ri.size() * 2, cudaMemcpyHostToDevice));
+        CSP_CUDA(cudaMemcpy(drc, rc.data(), rc.size() * 2, cudaMemcpyHostToDevice));
+        ld.rp_idx = dri;
+        ld.rp_cnt = drc;
+        ld.rp_w = h.vals[0];
+    }
     if (net.dev.kernel == COSPDNN_KERNEL_TCGEN05) {
         int rc = tc_build_blocks(h.colptr, h.rowidx, h.vals, N, net.d.precision, ld, e->owned);
         if (rc) return rc;

@@ -39,6 +39,12 @@ struct LayerDev {
     const int32_t *ell_idx;
     const float *ell_val;
     int K;
+    // The same entries for the FP64 replay when every weight of the layer
+    // has one FP32 value and N <= 65536: 16-bit input indices [K][N] (real
+    // entries only, ascending, rp_cnt[j] of them) and that value.
+    const uint16_t *rp_idx;
+    const uint16_t *rp_cnt;
+    float rp_w;
     // tcgen05 schedule (16x16 aligned blocks of W, built by tc_build_blocks):
     // output block columns are taken in chunks of up to 32 (one TMEM
     // accumulator of 16 columns each); within a chunk the MMAs are ordered by

@@ -234,9 +234,32 @@ __device__ void replay_row(const NetDev &nd, int p, double *buf0, double *buf1, 
     for (int ll = 0; ll <= l; ++ll) {
         const LayerDev &lw = nd.layers[ll];
         for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            double acc = 0.0;
+            if (lw.rp_idx) {
+                // one weight value: 16-bit indices of the real entries only
+                const double w = (double)lw.rp_w;
+                const int c = lw.rp_cnt[j];
+                const uint16_t *ip = lw.rp_idx + j;
+                int k = 0;
+                for (; k + 32 <= c; k += 32) {
+                    uint32_t ii[32];
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) ii[t] = __ldg(ip + (int64_t)(k + t) * N);
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) {
+                        const double yi = y[ii[t]];
+                        if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn(w, yi));
+                    }
+                }
+                for (; k < c; ++k) {
+                    const double yi = y[__ldg(ip + (int64_t)k * N)];
+                    if (yi != 0.0) acc = __dadd_rn(acc, __dmul_rn(w, yi));
+                }
+                z[j] = clamp32d(__dadd_rn(acc, b));
+                continue;
+            }
             // entries in ascending input order, loads issued 8 ahead of the
             // (strictly sequential) accumulation
-            double acc = 0.0;
             const int32_t *ip = lw.ell_idx + j;
             const float *wp = lw.ell_val + j;
             int k = 0;
