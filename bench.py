@@ -82,6 +82,7 @@ DRAM_BYTES_PER_ROW = {
     "c1": (135.193088e6 + 88.413696e6) / 32768,  # k_layer_cc_1024n_32768rows_fp32.md
     "c3": (271.177216e6 + 224.850688e6) / 8192,  # k_layer_cc_16384n_8192rows_bf16.md
     "r1": (134.869248e6 + 83.793152e6) / 16384,  # k_layer_tc_4096n_16384rows_r1_fp16.md
+    "c4": (280.101632e6 + 228.839424e6) / 2048,  # k_layer_cs_65536n_2048rows_fp16.md
 }
 
 def measured_peaks():
@@ -462,11 +463,16 @@ def main():
     ap.add_argument("--no-reference-build", action="store_true",
                     help="--impl reference: skip timing the reference's own CUDA build")
     ap.add_argument("--rows", type=int, default=None, help="override the rows per network (profiling)")
+    ap.add_argument("--layers", type=int, default=None,
+                    help="override the layers per network (profiling: the XOR-mask configurations have no "
+                         "rows left after a few layers, and the device loop stops there)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     nets, prec, dens = config_nets(args.config)
     if args.rows:
         nets = [(n, l, args.rows) for n, l, _ in nets]
+    if args.layers:
+        nets = [(n, args.layers, b) for n, _, b in nets]
     if args.precision:
         prec = args.precision
     if args.impl == "reference":
