@@ -89,6 +89,17 @@ def greedy_blocks(rows, cols, neuron, block=BLOCK):
     return int(nstart.sum())
 
 
+def mma_regions(colptr, rowidx, neuron, k=16, n=16):
+    """Number of aligned k x n regions (k inputs x n outputs) holding a
+    non-zero of one layer (CSC over input rows x outputs): the MMAs that a
+    tensor-core layer kernel of MMA depth k and width n issues per row tile,
+    whatever the fill of each region."""
+    colptr = np.asarray(colptr, np.int64)
+    rows = np.asarray(rowidx, np.int64)
+    cols = np.repeat(np.arange(neuron, dtype=np.int64), np.diff(colptr))
+    return int(np.unique((rows // k) * (neuron // n + 1) + cols // n).size)
+
+
 def similarity_order(rows, cols, neuron, block=BLOCK, seed=0, align=True):
     """Row order (new position -> original row) grouping rows by the output
     block columns they feed.  With `align`, every group of rows with equal

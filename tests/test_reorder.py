@@ -148,3 +148,21 @@ def test_main_reports_missing_or_damaged_files(tmp_path, capsys):
     assert ro.main([str(tmp_path / "src"), str(tmp_path / "out"), str(n), "2", "--workers", "1"]) == 1
     assert "index out of range" in capsys.readouterr().out
 
+
+
+def test_mma_regions_counts_aligned_regions():
+    from cospdnn_b200 import synth
+    # hand-made: output 0 <- inputs 0 and 17, output 20 <- input 3 (N = 32)
+    colptr = np.zeros(33, np.int64)
+    colptr[1:] = 2
+    colptr[21:] = 3
+    rowidx = np.array([0, 17, 3])
+    assert ro.mma_regions(colptr, rowidx, 32, 16, 16) == 3   # (0,0) (1,0) (0,1)
+    assert ro.mma_regions(colptr, rowidx, 32, 16, 32) == 2   # (0,0) (1,0)
+    assert ro.mma_regions(colptr, rowidx, 32, 32, 32) == 1
+    # two dense aligned 16x16 blocks per block column
+    cp, ri, _ = synth.masks_to_csc(synth.r1_masks(7, 0, 0, 256), 256)
+    assert ro.mma_regions(cp, ri, 256, 16, 16) == 2 * 256 // 16
+    # XOR masks: both 8-output halves of a 16-output group read the same input blocks
+    cp, ri, _ = synth.masks_to_csc(synth.xor_masks(7, 0, 0, 1024), 1024)
+    assert ro.mma_regions(cp, ri, 1024, 16, 8) == 2 * ro.mma_regions(cp, ri, 1024, 16, 16)
