@@ -143,6 +143,25 @@ def weight_bytes(info, n, prec):
     return 32.0 * n * 8      # int32 index + float weight per entry
 
 
+def own_bound(names, prec, fma_per_launch, ms_per_launch, sms, sm_mhz):
+    """The dominant CUDA-core layer kernel against its own bound: one 128-byte
+    shared-load wavefront per clock per SM.  A wavefront carries 64 FMAs of
+    16-bit rows (16- or 8-byte lanes of 8 or 4 rows; the feature-split
+    kernel's 4-byte words of 2 rows) and 32 of FP32 rows.  Counts the
+    algorithmic FMAs (one per non-zero weight and active row), not the
+    zero-weight padding of the conflict-free schedule.  None for the other
+    kernels (tcgen05, row-major gather) or without a time."""
+    if not names or ms_per_launch <= 0 or sms <= 0 or sm_mhz <= 0:
+        return None
+    if not all(n.startswith(("k_layer_cc<", "k_layer_cs<")) for n in names):
+        return None
+    peak = 32.0 if prec == "fp32" else 64.0
+    achieved = fma_per_launch / (ms_per_launch * 1e-3) / (sms * sm_mhz * 1e6)
+    return {"bound": "shared-memory wavefronts (one 128-byte wavefront per clock per SM)",
+            "achieved": achieved, "peak": peak, "unit": "FMA/clk/SM", "frac": achieved / peak,
+            "fma_per_launch": fma_per_launch, "sms": sms, "sm_mhz": sm_mhz}
+
+
 class Clocks:
     """nvidia-smi samples during the timed region."""
 
@@ -351,6 +370,45 @@ def reference_cuda_build(nets, kind, dens):
                       "R1 weights: two aligned dense blocks per block column, computed in full."))}
 
 
+def _ref_build_child(q, nets, kind, dens):
+    try:
+        q.put(reference_cuda_build(nets, kind, dens))
+    except Exception as ex:
+        q.put({"unavailable": f"{type(ex).__name__}: {ex}"})
+
+
+def reference_cuda_build_isolated(nets, kind, dens, timeout_s=600.0):
+    """reference_cuda_build in a child process (spawned): the reference's host
+    code ends its process on any CUDA error (Safe_Call -> exit,
+    src/gpu_lib/gpu_runtime.h:6-17), which must not take this arm's line
+    with it.  Bounded by timeout_s."""
+    import multiprocessing as mp
+    import queue
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_ref_build_child, args=(q, nets, kind, dens), daemon=True)
+    p.start()
+    t_end = time.time() + timeout_s
+    res = None
+    while res is None and time.time() < t_end:
+        try:
+            res = q.get(timeout=1.0)
+        except queue.Empty:
+            if not p.is_alive():
+                try:
+                    res = q.get(timeout=1.0)
+                except queue.Empty:
+                    break
+    p.join(10)
+    if p.is_alive():
+        p.kill()
+        p.join()
+    if res is None:
+        return {"unavailable": f"the reference's host code ended without a result (exit status {p.exitcode}: "
+                               f"it exits on a CUDA error, or ran over {timeout_s:.0f} s)"}
+    return res
+
+
 def run_reference(args, nets, prec, dens):
     """--impl reference: the CPU implementation of the recurrence, timed here."""
     rank = int(os.environ.get("RANK", "0"))
@@ -387,10 +445,8 @@ def run_reference(args, nets, prec, dens):
     sample = ", ".join(f"{rows} of {nets[i][2]} rows of net {i}" for i, rows, _, _ in samples)
     ref_build = None
     if not args.no_reference_build:
-        try:
-            ref_build = reference_cuda_build(nets, weight_kind(args.config), dens)
-        except Exception as ex:  # reported, not fatal: the arm's value is the CPU port
-            ref_build = {"unavailable": f"{type(ex).__name__}: {ex}"}
+        # reported, not fatal: the arm's value is the CPU port
+        ref_build = reference_cuda_build_isolated(nets, weight_kind(args.config), dens)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -539,7 +595,8 @@ def main():
     b_l0 = np.zeros(nit)
     b_ly = np.zeros(nit)
     rows_ly = np.zeros(nit)
-    for r, info, (n, L, b) in zip(results, infos, nets):
+    fma_ly = np.zeros(nit)
+    for r, info, (n, L, b), w in zip(results, infos, nets, weights):
         rows_in = np.concatenate([[b], r["alive"][:-1]])
         for it in range(min(nit, L)):
             R = float(rows_in[it])
@@ -552,6 +609,7 @@ def main():
                 # active input rows read, their outputs written, W
                 b_ly[it] += 2.0 * R * n * es + weight_bytes(info, n, prec)
                 rows_ly[it] += R
+                fma_ly[it] += R * float(w[it][0][-1])  # nnz(W_l) FMAs per active row
     # iteration 0 is the counting kernel when every net counted layer 0
     l0_iter = all(i["layer0_counted"] for i in infos)
     t_l0 = float(lms[0]) if (nit and l0_iter) else 0.0
@@ -590,6 +648,16 @@ def main():
                             "frac": float(b_l0[0] / (t_l0 * 1e-3) / 1e9 / peak) if t_l0 > 0 else 0.0}
                            if l0_iter else None),
                 "per_layer": per_layer}
+    if not dominant_is_l0:
+        # a secondary figure: it must not cost the line when a clock sample is odd
+        try:
+            csum = clk.summary() or {}
+            roofline["own_bound"] = own_bound(
+                names, prec, float(sum(fma_ly[i] for i in it_ly)) / max(1, len(it_ly)), kt / klaunch,
+                torch.cuda.get_device_properties(local).multi_processor_count,
+                float(csum.get("sm_mhz") or csum.get("sm_max_mhz") or 0.0))
+        except (TypeError, ValueError, KeyError) as ex:
+            roofline["own_bound"] = {"error": repr(ex)}
 
     # ---- end to end through the public API: pinned host Y0 -> H2D -> run -> D2H result
     e2e = None
