@@ -54,11 +54,12 @@ def build(force=False, verbose=False):
 
 
 CLI = os.path.join(HERE, "cli")
-CLI_PROGRAMS = ["cospdnn", "cospdnn_double"]
+CLI_PROGRAMS = ["cospdnn", "cospdnn_double", "cospdnn_multi"]
 
 
 def build_cli(force=False):
-    """The reference's command lines (cli/cospdnn.out, cli/cospdnn_double.out):
+    """The reference's command lines (cli/cospdnn.out, cli/cospdnn_double.out) and
+    their k-network form (cli/cospdnn_multi.out):
     host C++ over the C ABI, linked against the in-tree library."""
     cxx = shutil.which("g++") or "g++"
     inc = os.path.join(os.path.dirname(HERE), "include")

@@ -30,6 +30,36 @@ def test_cli_usage(name, nargs):
     assert out.stdout.startswith("Usage: exe neuron")
 
 
+@pytest.mark.parametrize("nargs", [1, 4, 7])
+def test_cli_multi_usage(nargs):
+    """cospdnn_multi.out takes three numbers per network, then gpu_id and
+    dataset_dir: any other count prints the usage line."""
+    out = subprocess.run([_exe("cospdnn_multi")] + ["1"] * nargs, capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0
+    assert out.stdout.startswith("Usage: exe neuron1 batch1 layer1 [neuron2 batch2 layer2 ...]")
+
+
+def test_cli_multi_fails_without_a_device(tmp_path):
+    """Three networks (two widths, one read twice) are parsed and cached; with
+    no CUDA device visible the run then ends with an error, not a result."""
+    from cospdnn_b200 import synth
+    for n, seed in ((64, 5), (128, 6)):
+        csc, y0, _ = make_net(n, 2, 10, seed=seed, dlo=0.2, dhi=0.4)
+        synth.write_reference_dataset(str(tmp_path / "d"), n, 2, y0, csc)
+    (tmp_path / "c").mkdir()
+    out = subprocess.run([_exe("cospdnn_multi"), "64", "10", "2", "128", "10", "2", "64", "8", "2", "0",
+                          str(tmp_path / "d")], capture_output=True, text=True, timeout=120,
+                         env=dict(os.environ, CUDA_VISIBLE_DEVICES="", COSPDNN_CACHE=str(tmp_path / "c")))
+    assert out.returncode != 0
+    assert "[Neuron3] :64" in out.stdout and "Total Kernel Exec Time" not in out.stdout
+    assert (tmp_path / "c" / "cospdnn-n64-b10-l2.bin").stat().st_size > 0
+    assert (tmp_path / "c" / "cospdnn-n128-b10-l2.bin").stat().st_size > 0
+    # a zero or negative size is rejected before any file is read
+    out = subprocess.run([_exe("cospdnn_multi"), "64", "10", "2", "128", "0", "2", "0", str(tmp_path / "d")],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode != 0 and "bad arguments" in out.stdout
+
+
 @pytest.mark.parametrize("gpu_num", [1, 2])
 def test_cli_fails_without_a_device(tmp_path, gpu_num):
     """With no CUDA device visible the program exits with an error for one
